@@ -1,0 +1,96 @@
+"""Build the sm_100a shared library and the harness-format runner in-tree.
+
+    python build.py            # incremental
+    python build.py --clean    # from scratch
+
+Outputs (git-ignored, shipped with the tree):
+    lib/libnegacyclic_b200.so   C ABI (include/negacyclic_b200.h) + fherma_init/run/free
+    bin/solution                harness runner: reads a case directory, writes out/*/c.bin
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+OBJ = PKG / "_build"
+LIB = PKG / "lib" / "libnegacyclic_b200.so"
+BIN = PKG / "bin" / "solution"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", f"-I{INCLUDE}", f"-I{CSRC}"]
+
+LIB_SOURCES = ["hostmath.cpp", "kernels.cu", "batch.cu", "engine.cu", "server.cu", "api.cu"]
+RUNNER_SOURCES = ["runner.cpp"]
+
+
+def _headers() -> list[Path]:
+    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def _compile(src: Path, verbose: bool) -> Path:
+    obj = OBJ / (src.name + ".o")
+    if not _stale(obj, [src] + _headers()):
+        return obj
+    cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
+    if src.suffix == ".cu" and verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if verbose and r.stderr:
+        (OBJ / (src.name + ".ptxas.txt")).write_text(r.stderr)
+    return obj
+
+
+def build(clean: bool = False, verbose: bool = False) -> Path:
+    if clean and OBJ.exists():
+        shutil.rmtree(OBJ)
+    OBJ.mkdir(parents=True, exist_ok=True)
+    LIB.parent.mkdir(parents=True, exist_ok=True)
+    BIN.parent.mkdir(parents=True, exist_ok=True)
+    sources = [CSRC / s for s in LIB_SOURCES if (CSRC / s).exists()]
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose), sources))
+    if _stale(LIB, objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    runner = [CSRC / s for s in RUNNER_SOURCES if (CSRC / s).exists()]
+    if runner and _stale(BIN, runner + [LIB] + _headers()):
+        cmd = ["g++", "-O2", "-std=c++17", f"-I{INCLUDE}", *map(str, runner), "-o", str(BIN),
+               f"-L{LIB.parent}", "-lnegacyclic_b200", f"-Wl,-rpath,$ORIGIN/../lib"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"runner link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--clean", action="store_true")
+    ap.add_argument("--verbose", action="store_true", help="keep ptxas register/spill reports in _build/")
+    a = ap.parse_args()
+    print(build(a.clean, a.verbose))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

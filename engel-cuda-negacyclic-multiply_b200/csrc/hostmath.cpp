@@ -1,0 +1,308 @@
+// Host-side precompute for the negacyclic product (see hostmath.h).
+#include "hostmath.h"
+
+#include <algorithm>
+#include <mutex>
+#include <thread>
+
+namespace nc {
+
+using u128 = unsigned __int128;
+
+uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t p) { return uint64_t((u128(a) * b) % p); }
+
+uint64_t powmod64(uint64_t a, uint64_t e, uint64_t p) {
+    uint64_t r = 1 % p;
+    a %= p;
+    while (e) {
+        if (e & 1) r = mulmod64(r, a, p);
+        a = mulmod64(a, a, p);
+        e >>= 1;
+    }
+    return r;
+}
+
+// Deterministic Miller-Rabin for 64-bit integers: the first twelve primes as bases.
+bool is_prime64(uint64_t n) {
+    if (n < 2) return false;
+    static const uint64_t small[] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+    for (uint64_t s : small) {
+        if (n % s == 0) return n == s;
+    }
+    uint64_t d = n - 1;
+    int r = 0;
+    while ((d & 1) == 0) {
+        d >>= 1;
+        ++r;
+    }
+    for (uint64_t a : small) {
+        uint64_t x = powmod64(a, d, n);
+        if (x == 1 || x == n - 1) continue;
+        bool composite = true;
+        for (int i = 1; i < r; ++i) {
+            x = mulmod64(x, x, n);
+            if (x == n - 1) {
+                composite = false;
+                break;
+            }
+        }
+        if (composite) return false;
+    }
+    return true;
+}
+
+int bit_length(const uint32_t* v, int L) {
+    for (int i = L - 1; i >= 0; --i)
+        if (v[i]) return i * 32 + 32 - __builtin_clz(v[i]);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------- big integers
+
+namespace {
+
+using Big = std::vector<uint32_t>;  // little-endian words, no fixed length
+
+void trim(Big& a) {
+    while (!a.empty() && a.back() == 0) a.pop_back();
+}
+
+int bits_of(const Big& a) { return bit_length(a.data(), int(a.size())); }
+
+Big mul_u64(const Big& a, uint64_t f) {
+    Big r(a.size() + 3, 0);
+    const uint64_t f0 = uint32_t(f), f1 = f >> 32;
+    for (size_t pass = 0; pass < 2; ++pass) {
+        const uint64_t fv = pass ? f1 : f0;
+        uint64_t carry = 0;
+        for (size_t i = 0; i < a.size(); ++i) {
+            const u128 cur = u128(r[i + pass]) + u128(a[i]) * fv + carry;
+            r[i + pass] = uint32_t(cur);
+            carry = uint64_t(cur >> 32);
+        }
+        for (size_t i = a.size() + pass; carry && i < r.size(); ++i) {
+            const uint64_t cur = uint64_t(r[i]) + carry;
+            r[i] = uint32_t(cur);
+            carry = cur >> 32;
+        }
+    }
+    trim(r);
+    return r;
+}
+
+// a / d exactly (remainder discarded) and a mod d.
+Big div_u64(const Big& a, uint64_t d, uint64_t* rem) {
+    Big q(a.size(), 0);
+    u128 r = 0;
+    for (int i = int(a.size()) - 1; i >= 0; --i) {
+        r = (r << 32) | a[i];
+        q[i] = uint32_t(r / d);
+        r %= d;
+    }
+    if (rem) *rem = uint64_t(r);
+    trim(q);
+    return q;
+}
+
+int cmp_shifted(const Big& a, const Big& b, int shift) {
+    // compare a with b << shift
+    const int words = int(std::max(a.size(), b.size() + size_t(shift / 32) + 1));
+    for (int i = words - 1; i >= 0; --i) {
+        const int w = shift >> 5, s = shift & 31;
+        uint32_t bv = 0;
+        const int src = i - w;
+        if (src >= 0 && src < int(b.size())) bv = b[src] << s;
+        if (s && src - 1 >= 0 && src - 1 < int(b.size())) bv |= b[src - 1] >> (32 - s);
+        const uint32_t av = i < int(a.size()) ? a[i] : 0;
+        if (av != bv) return av > bv ? 1 : -1;
+    }
+    return 0;
+}
+
+void sub_shifted(Big& a, const Big& b, int shift) {
+    const int w = shift >> 5, s = shift & 31;
+    int64_t borrow = 0;
+    for (size_t i = 0; i < a.size(); ++i) {
+        uint32_t bv = 0;
+        const int src = int(i) - w;
+        if (src >= 0 && src < int(b.size())) bv = b[src] << s;
+        if (s && src - 1 >= 0 && src - 1 < int(b.size())) bv |= b[src - 1] >> (32 - s);
+        const int64_t cur = int64_t(a[i]) - bv - borrow;
+        a[i] = uint32_t(cur);
+        borrow = cur < 0 ? 1 : 0;
+    }
+    trim(a);
+}
+
+// a mod m and (optionally) floor(a / m), by shift-and-subtract.
+Big divmod(Big a, const Big& m, Big* quot) {
+    trim(a);
+    const int mb = bits_of(m);
+    int ab = bits_of(a);
+    Big q;
+    if (quot) q.assign(a.size() + 1, 0);
+    for (int shift = ab - mb; shift >= 0; --shift) {
+        if (cmp_shifted(a, m, shift) >= 0) {
+            sub_shifted(a, m, shift);
+            if (quot) q[shift >> 5] |= 1u << (shift & 31);
+        }
+    }
+    if (quot) {
+        trim(q);
+        *quot = q;
+    }
+    return a;
+}
+
+Big pow2(int e) {
+    Big r(size_t(e / 32 + 1), 0);
+    r[e / 32] = 1u << (e % 32);
+    return r;
+}
+
+uint32_t bitrev(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int i = 0; i < bits; ++i) r |= ((x >> i) & 1u) << (bits - 1 - i);
+    return r;
+}
+
+std::vector<PrimeConst> make_prime_set() {
+    std::vector<PrimeConst> out;
+    const uint64_t step = 1ull << kRootLog;
+    uint64_t cand = (1ull << 62) - step + 1;
+    while (int(out.size()) < kMaxPrimes) {
+        if (is_prime64(cand)) {
+            PrimeConst c{};
+            c.p = cand;
+            c.m = (1ull << 62) - cand;
+            c.g = uint32_t((u128(1) << 93) / cand);
+            out.push_back(c);
+        }
+        cand -= step;
+    }
+    return out;
+}
+
+}  // namespace
+
+const std::vector<PrimeConst>& prime_set() {
+    static const std::vector<PrimeConst> set = make_prime_set();
+    return set;
+}
+
+int primes_needed(int logN, int qbits) {
+    const int bound_bits = logN + 2 * qbits + 4;
+    Big prod{1};
+    const auto& ps = prime_set();
+    for (int k = 1; k <= kMaxPrimes; ++k) {
+        prod = mul_u64(prod, ps[k - 1].p);
+        if (bits_of(prod) >= bound_bits) return k;
+    }
+    return -1;
+}
+
+const HostTables& host_tables() {
+    static HostTables t;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        t.pc = prime_set();
+        t.psi.assign(kMaxPrimes, 0);
+        t.pow32.assign(size_t(kMaxPrimes) * kMaxL, 0);
+        t.fwd.assign(size_t(kMaxPrimes) * kMaxN * 2, 0);
+        t.inv.assign(size_t(kMaxPrimes) * kMaxN * 2, 0);
+        auto work = [](int i) {
+            const uint64_t p = t.pc[i].p;
+            // psi of multiplicative order 2^17: g^((p-1)/2^17) with psi^(2^16) = -1
+            uint64_t psi = 0;
+            for (uint64_t g = 2; g < 1000000; ++g) {
+                const uint64_t c = powmod64(g, (p - 1) >> kRootLog, p);
+                if (powmod64(c, 1ull << kMaxLogN, p) == p - 1) {
+                    psi = c;
+                    break;
+                }
+            }
+            t.psi[i] = psi;
+            uint64_t place = 1;
+            for (int l = 0; l < kMaxL; ++l) {
+                t.pow32[size_t(i) * kMaxL + l] = place;
+                place = mulmod64(place, 1ull << 32, p);
+            }
+            std::vector<uint64_t> pw(kMaxN + 1);
+            pw[0] = 1;
+            for (int e = 1; e <= kMaxN; ++e) pw[e] = mulmod64(pw[e - 1], psi, p);
+            // pw[kMaxN] = -1, so psi^-e = -psi^(kMaxN - e)
+            uint64_t* f = t.fwd.data() + size_t(i) * kMaxN * 2;
+            uint64_t* g = t.inv.data() + size_t(i) * kMaxN * 2;
+            for (uint32_t j = 0; j < uint32_t(kMaxN); ++j) {
+                const uint32_t e = bitrev(j, kMaxLogN);
+                const uint64_t w = pw[e];
+                const uint64_t wi = e == 0 ? 1 : p - pw[kMaxN - e];
+                f[2 * j] = w;
+                f[2 * j + 1] = uint64_t((u128(w) << 64) / p);
+                g[2 * j] = wi;
+                g[2 * j + 1] = uint64_t((u128(wi) << 64) / p);
+            }
+        };
+        const int nthreads = std::max(1, std::min<int>(16, int(std::thread::hardware_concurrency())));
+        std::vector<std::thread> pool;
+        for (int w = 0; w < nthreads; ++w)
+            pool.emplace_back([&, w] {
+                for (int i = w; i < kMaxPrimes; i += nthreads) work(i);
+            });
+        for (auto& th : pool) th.join();
+    });
+    return t;
+}
+
+std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out) {
+    if (L < 1 || L > kMaxL) return "L must be between 1 and 32";
+    if (logN < 1 || logN > kMaxLogN) return "N must be a power of two from 2 to 65536";
+    if ((q[0] & 1u) == 0) return "q must be odd";
+    const int qbits = bit_length(q, L);
+    if (qbits <= 32 * (L - 1)) return "the top limb of q must be nonzero";
+    const int k = primes_needed(logN, qbits);
+    if (k < 0) return "the coefficient bound does not fit the 48-prime residue budget";
+    const auto& ps = prime_set();
+
+    *out = QConst{};
+    out->L = uint32_t(L);
+    out->LW = uint32_t((L + 1) & ~1);
+    out->k = uint32_t(k);
+    out->qbits = uint32_t(qbits);
+    out->logN = uint32_t(logN);
+    Big qb(q, q + L);
+    trim(qb);
+    for (int l = 0; l < L; ++l) out->q[l] = q[l];
+
+    Big M{1};
+    for (int i = 0; i < k; ++i) M = mul_u64(M, ps[i].p);
+    const uint64_t N = 1ull << logN;
+    for (int i = 0; i < k; ++i) {
+        const uint64_t p = ps[i].p;
+        uint64_t rem = 0;
+        const Big Mi = div_u64(M, p, &rem);
+        uint64_t mi_mod_p = 0;
+        div_u64(Mi, p, &mi_mod_p);
+        // y = (M/p_i)^-1 * N^-1 mod p_i
+        const uint64_t inv_mi = powmod64(mi_mod_p, p - 2, p);
+        const uint64_t inv_n = powmod64(N % p, p - 2, p);
+        const uint64_t y = mulmod64(inv_mi, inv_n, p);
+        out->y[i] = y;
+        out->ys[i] = uint64_t((u128(y) << 64) / p);
+        const Big miq = divmod(Mi, qb, nullptr);
+        for (size_t l = 0; l < miq.size() && l < size_t(kMqStride); ++l) out->mq[i * kMqStride + l] = miq[l];
+    }
+    const Big mmq = divmod(M, qb, nullptr);
+    Big neg = qb;
+    if (!mmq.empty()) sub_shifted(neg, mmq, 0);
+    else neg.clear();  // M = 0 mod q cannot happen for prime q > 2^62, kept for completeness
+    if (bits_of(neg) == bits_of(qb) && cmp_shifted(neg, qb, 0) == 0) neg.clear();
+    for (size_t l = 0; l < neg.size(); ++l) out->neg_m[l] = neg[l];
+    Big mu;
+    divmod(pow2(qbits + kBarrettT + 1), qb, &mu);
+    if (bits_of(mu) > 96) return "internal: Barrett constant too wide";
+    for (size_t l = 0; l < mu.size() && l < 4; ++l) out->mu[l] = mu[l];
+    return std::string();
+}
+
+}  // namespace nc

@@ -1,0 +1,43 @@
+// Host-side precompute: the fixed prime set, twiddle tables and per-(q, N) CRT constants.
+// This is the planning half of the reference's fherma_init (solve.cu:1150-1487), redone with
+// 128-bit integer division instead of bit-serial loops, and for a prime set shared by all N.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "common.h"
+
+namespace nc {
+
+struct HostTables {
+    std::vector<PrimeConst> pc;          // kMaxPrimes
+    std::vector<uint64_t> psi;           // primitive 2^17-th root of unity per prime
+    std::vector<uint64_t> pow32;         // kMaxPrimes * kMaxL
+    std::vector<uint64_t> fwd;           // kMaxPrimes * kMaxN * 2 (w, shoup)
+    std::vector<uint64_t> inv;           // same for psi^-1
+};
+
+// Built once per process (thread-safe); about 100 MB of host memory.
+const HostTables& host_tables();
+
+// The primes only (cheap; no twiddles).
+const std::vector<PrimeConst>& prime_set();
+
+// Bit length of an L-limb value (0 for zero).
+int bit_length(const uint32_t* v, int L);
+
+// Number of primes of the set needed for ring degree 2^logN and a qbits-bit modulus, by the
+// reference's bound bitlen(prod p) >= logN + 2 qbits + 4 (solve.cu:1177-1204); -1 if > 48.
+int primes_needed(int logN, int qbits);
+
+// Fill the CRT + Barrett constants. Returns an empty string or an error message.
+std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out);
+
+// Small helpers shared with the tests of the host math.
+uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t p);
+uint64_t powmod64(uint64_t a, uint64_t e, uint64_t p);
+bool is_prime64(uint64_t n);
+
+}  // namespace nc

@@ -1,0 +1,216 @@
+"""Python binding of libnegacyclic_b200.so (ctypes over the C ABI in include/negacyclic_b200.h).
+
+The functions fherma_init / fherma_run / fherma_free mirror the reference's C++ contract
+(fherma.h:45-47): same names, same argument meaning (Point{N, W, L, q}, Inputs{a, b},
+Outputs{c} with N x L little-endian u32 limbs) and the same error behaviour (a RuntimeError
+with a message where the reference throws std::runtime_error).
+
+There is no fallback: if the shared library is missing or fails to load, every entry point
+raises. Build it with `python build.py` in this directory.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "lib" / "libnegacyclic_b200.so"
+
+NC_OK, NC_EINVAL, NC_ECUDA, NC_ENOMEM, NC_ETIMEOUT, NC_EBUSY = 0, -1, -2, -3, -4, -5
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_vp = ctypes.c_void_p
+
+# (name, restype, argtypes) of every symbol include/negacyclic_b200.h declares.
+C_SYMBOLS = [
+    ("nc_last_error", ctypes.c_char_p, []),
+    ("nc_version", ctypes.c_int, []),
+    ("nc_plan_create", ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.POINTER(_vp)]),
+    ("nc_plan_destroy", ctypes.c_int, [_vp]),
+    ("nc_multiply", ctypes.c_int, [_vp, _u32p, _u32p, _u32p]),
+    ("nc_multiply_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    ("nc_plan_synchronize", ctypes.c_int, [_vp]),
+    ("nc_plan_query", ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _u32p]),
+    ("nc_plan_last_kernel_ms", ctypes.c_float, [_vp]),
+    ("nc_plan_set_timing", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nc_plan_stage_ms", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    ("nc_imad_peak", ctypes.c_int, [ctypes.POINTER(ctypes.c_double)]),
+    ("nc_primes", ctypes.c_int, [_u64p, ctypes.c_int]),
+]
+
+_lib: ctypes.CDLL | None = None
+
+
+class NegacyclicError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{message} (status {code})")
+        self.code = code
+
+
+def load(path: str | Path | None = None) -> ctypes.CDLL:
+    """Load the library (once) and declare every C entry point."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: build it with `python build.py` (no CPU fallback exists)")
+    lib = ctypes.CDLL(str(p))
+    for name, res, args in C_SYMBOLS:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != NC_OK:
+        msg = load().nc_last_error().decode(errors="replace")
+        raise NegacyclicError(status, msg)
+
+
+def _u32(arr: np.ndarray):
+    return arr.ctypes.data_as(_u32p)
+
+
+def imad_peak() -> float:
+    """Measured mad.lo.u32 throughput of the current device (ops/s)."""
+    v = ctypes.c_double()
+    _check(load().nc_imad_peak(ctypes.byref(v)))
+    return float(v.value)
+
+
+def primes(count: int = 48) -> list[int]:
+    out = (ctypes.c_uint64 * count)()
+    _check(load().nc_primes(out, count))
+    return list(out)
+
+
+class Plan:
+    """One (N, q) configuration on the current CUDA device."""
+
+    def __init__(self, N: int, q_limbs: np.ndarray, W: int = 0):
+        q = np.ascontiguousarray(q_limbs, dtype=np.uint32)
+        self.N, self.L = int(N), int(q.size)
+        self._h = _vp()
+        _check(load().nc_plan_create(self.N, int(W), self.L, _u32(q), ctypes.byref(self._h)))
+        n, l, k, qb = (ctypes.c_uint32() for _ in range(4))
+        _check(load().nc_plan_query(self._h, ctypes.byref(n), ctypes.byref(l), ctypes.byref(k), ctypes.byref(qb)))
+        self.k, self.qbits = int(k.value), int(qb.value)
+
+    @property
+    def handle(self) -> int:
+        return int(self._h.value or 0)
+
+    def multiply(self, a: np.ndarray, b: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        """Host arrays (N, L) u32 in, product out (nc_multiply: copies both ways)."""
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        b = np.ascontiguousarray(b, dtype=np.uint32)
+        if a.size != self.N * self.L or b.size != self.N * self.L:
+            raise NegacyclicError(NC_EINVAL, "a and b must contain N*L limbs")
+        c = out if out is not None else np.empty((self.N, self.L), dtype=np.uint32)
+        _check(load().nc_multiply(self._h, _u32(a), _u32(b), _u32(c)))
+        return c
+
+    def multiply_device(self, d_a: int, d_b: int, d_c: int, stream: int = 0) -> None:
+        """Device pointers (e.g. torch tensor .data_ptr()), enqueued on `stream` (0: default stream)."""
+        _check(load().nc_multiply_device(self._h, _vp(d_a), _vp(d_b), _vp(d_c), _vp(stream or None)))
+
+    def synchronize(self) -> None:
+        _check(load().nc_plan_synchronize(self._h))
+
+    def set_timing(self, enable: bool = True) -> None:
+        _check(load().nc_plan_set_timing(self._h, int(enable)))
+
+    def stage_ms(self) -> list[float]:
+        out = (ctypes.c_float * 3)()
+        _check(load().nc_plan_stage_ms(self._h, out))
+        return list(out)
+
+    @property
+    def last_kernel_ms(self) -> float:
+        return float(load().nc_plan_last_kernel_ms(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            _check(load().nc_plan_destroy(self._h))
+            self._h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ the reference's interface
+
+
+@dataclass
+class Tensor:
+    shape: list
+    data: np.ndarray
+
+    def count(self) -> int:
+        n = 1
+        for d in self.shape:
+            n *= int(d)
+        return n
+
+
+@dataclass
+class Point:
+    N: int
+    W: int
+    L: int
+    q: Tensor
+
+
+@dataclass
+class Inputs:
+    a: Tensor
+    b: Tensor
+
+
+@dataclass
+class Outputs:
+    c: Tensor = field(default_factory=lambda: Tensor([], np.zeros(0, dtype=np.uint32)))
+
+
+def fherma_init(p: Point) -> Plan:
+    """Setup for one point; raises RuntimeError on an invalid point (fherma.h:45)."""
+    q = np.ascontiguousarray(p.q.data, dtype=np.uint32).reshape(-1)
+    if q.size != p.L:
+        raise RuntimeError("q must hold L limbs")
+    return Plan(p.N, q, W=p.W)
+
+
+def fherma_run(state: Plan, inputs: Inputs) -> Outputs:
+    """c = a * b mod (X^N + 1, q); raises RuntimeError on bad sizes (fherma.h:46)."""
+    if state is None:
+        raise RuntimeError("null state")
+    count = state.N * state.L
+    a = np.ascontiguousarray(inputs.a.data, dtype=np.uint32).reshape(-1)
+    b = np.ascontiguousarray(inputs.b.data, dtype=np.uint32).reshape(-1)
+    if a.size != count or b.size != count:
+        raise RuntimeError("a and b must contain N*L limbs")
+    c = state.multiply(a.reshape(state.N, state.L), b.reshape(state.N, state.L))
+    return Outputs(Tensor([state.N, state.L], c.reshape(-1)))
+
+
+def fherma_free(state: Plan | None) -> None:
+    """Releases the state; None is a no-op (fherma.h:47)."""
+    if state is not None:
+        state.close()

@@ -1,0 +1,86 @@
+/*
+ * C ABI of the B200 negacyclic product library: c = a * b mod (X^N + 1, q).
+ *
+ * Every operand is N coefficients of L little-endian u32 limbs, coefficient-major
+ * (coefficient i at limbs [i*L, i*L + L)), values in [0, q). q is an odd L-limb modulus
+ * whose top limb is nonzero; N is a power of two from 2 to 65536.
+ *
+ * Each entry point returns NC_OK (0) or a negative status; nc_last_error() then returns a
+ * message for the calling thread. The C++ entry points of the reference's contract
+ * (fherma_init / fherma_run / fherma_free, declared in fherma.h) are exported by the same
+ * library and throw std::runtime_error instead.
+ */
+#ifndef NEGACYCLIC_B200_H
+#define NEGACYCLIC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    NC_OK = 0,
+    NC_EINVAL = -1,   /* bad argument: size, alignment, modulus, null pointer */
+    NC_ECUDA = -2,    /* a CUDA call failed */
+    NC_ENOMEM = -3,   /* device or pinned allocation failed, or an HBM budget is exceeded */
+    NC_ETIMEOUT = -4, /* a persistent-kernel dependency wait gave up (bounded spin) */
+    NC_EBUSY = -5     /* the object is in use (server full, request not finished) */
+};
+
+typedef struct nc_plan nc_plan;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* nc_last_error(void);
+
+/* Library version, major * 10000 + minor * 100 + patch. */
+int nc_version(void);
+
+/* ------------------------------------------------------------------ one product per call */
+
+/* Plan for one (N, q): tables, constants and scratch on the current device.
+   Replaces fherma_init (reference fherma.h:45, solve.cu:1150-1487). W is q's bit width as
+   the platform states it (L = (W + 31) / 32), or 0 to take it from q. Not reentrant: one
+   product at a time per plan. */
+int nc_plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, nc_plan** out);
+
+/* Releases the plan (null is a no-op). Replaces fherma_free (fherma.h:47, solve.cu:1530-1567). */
+int nc_plan_destroy(nc_plan* plan);
+
+/* Host buffers in and out, synchronous. Replaces fherma_run (fherma.h:46, solve.cu:1489-1528). */
+int nc_multiply(nc_plan* plan, const uint32_t* a, const uint32_t* b, uint32_t* c);
+
+/* Device-resident operands (16-byte aligned), enqueued on `stream` exactly as given (a
+   cudaStream_t; 0 is the CUDA default stream). Returns once enqueued. Uses the plan's scratch
+   residues, so calls on one plan must not overlap on the device. */
+int nc_multiply_device(nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream);
+
+/* Waits for the plan's own stream (the one nc_multiply uses). */
+int nc_plan_synchronize(nc_plan* plan);
+
+/* N, L, number of residue primes k, and bit length of q. Any pointer may be NULL. */
+int nc_plan_query(const nc_plan* plan, uint32_t* N, uint32_t* L, uint32_t* k, uint32_t* qbits);
+
+/* Device milliseconds of the kernels of the last nc_multiply (CUDA events). */
+float nc_plan_last_kernel_ms(const nc_plan* plan);
+
+/* Per-stage device timing of the plan's products: when enabled, each product records CUDA
+   events around its three kernels (residues + forward column stages; row NTTs + pointwise;
+   inverse column stages + CRT). nc_plan_stage_ms returns the three durations of the last
+   product once it has completed. */
+int nc_plan_set_timing(nc_plan* plan, int enable);
+int nc_plan_stage_ms(const nc_plan* plan, float* ms3);
+
+/* Measured 32-bit integer multiply-add throughput of the current device in ops/s (a chain of
+   mad.lo.u32 over every SM): the denominator of the IMAD roofline. Takes a few milliseconds. */
+int nc_imad_peak(double* ops_per_second);
+
+/* Residue primes of the fixed set (p = 2^62 - m, p = 1 mod 2^17), first `count` of 48. */
+int nc_primes(uint64_t* out, int count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEGACYCLIC_B200_H */

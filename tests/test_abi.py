@@ -1,0 +1,104 @@
+"""The C ABI library loads, exports every declared symbol and the reference's C++ contract, and
+rejects invalid points before touching a GPU. No compute calls here."""
+from __future__ import annotations
+
+import re
+import subprocess
+
+import pytest
+
+import negacyclic as nc
+from conftest import ROOT, has_gpu
+
+HEADER = ROOT / "include" / "negacyclic_b200.h"
+
+
+def declared_symbols() -> set[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(nc_[a-z0-9_]+)\s*\(", text))
+
+
+def test_library_loads():
+    lib = nc.load()
+    assert lib.nc_version() >= 100
+
+
+def test_every_declared_symbol_is_exported_and_bound():
+    lib = nc.load()
+    decl = declared_symbols()
+    assert decl, "no declarations parsed"
+    bound = {name for name, _, _ in nc.C_SYMBOLS}
+    assert decl == bound, f"header vs binding mismatch: {decl ^ bound}"
+    for name in decl:
+        assert hasattr(lib, name), name
+
+
+def test_reference_contract_symbols_exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", "-C", str(nc.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    assert "fherma_init(fherma::Point const&)" in out
+    assert "fherma_run(void*, fherma::Inputs const&)" in out
+    assert "fherma_free(void*)" in out
+
+
+@pytest.mark.parametrize("N,L,q,msg", [
+    (3, 1, [0xFFFFFFFB], "power of two"),
+    (0, 1, [0xFFFFFFFB], "power of two"),
+    (1 << 17, 1, [0xFFFFFFFB], "power of two"),
+    (8, 0, [], "L must"),
+    (8, 33, [1] * 33, "L must"),
+    (8, 1, [10], "odd"),
+    (8, 2, [7, 0], "top limb"),
+])
+def test_invalid_points_rejected(N, L, q, msg):
+    import numpy as np
+
+    arr = np.array(q if q else [0], dtype=np.uint32)
+    lib = nc.load()
+    import ctypes
+
+    h = ctypes.c_void_p()
+    st = lib.nc_plan_create(N, 0, L, arr.ctypes.data_as(nc._u32p), ctypes.byref(h))
+    assert st == nc.NC_EINVAL
+    assert msg in lib.nc_last_error().decode()
+    assert not h.value
+
+
+def test_width_must_match_limbs():
+    import numpy as np
+
+    q = np.array([0xFFFFFFFB, 1], dtype=np.uint32)
+    with pytest.raises(nc.NegacyclicError, match="W must"):
+        nc.Plan(8, q, W=100)
+
+
+def test_null_arguments():
+    lib = nc.load()
+    assert lib.nc_plan_create(8, 0, 1, None, None) == nc.NC_EINVAL
+    assert lib.nc_multiply(None, None, None, None) == nc.NC_EINVAL
+    assert lib.nc_plan_destroy(None) == nc.NC_OK
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-GPU failure mode")
+def test_valid_point_without_gpu_fails_loudly():
+    import numpy as np
+
+    q = np.array([0xFFFFFFFB], dtype=np.uint32)  # 2^32 - 5, prime
+    with pytest.raises(nc.NegacyclicError) as ei:
+        nc.Plan(8, q)
+    assert ei.value.code in (nc.NC_ECUDA, nc.NC_ENOMEM)
+
+
+def test_prime_set():
+    import random
+
+    import cases
+
+    ps = nc.primes(48)
+    assert len(ps) == 48 and ps == sorted(ps, reverse=True)
+    rng = random.Random(1)
+    for p in ps:
+        assert p < (1 << 62) and p % (1 << 17) == 1
+        assert (1 << 62) - p < (1 << 28)
+        assert cases.is_probable_prime(p, 16, rng)
