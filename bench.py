@@ -1,0 +1,427 @@
+#!/usr/bin/env python
+"""Benchmark of the negacyclic product c = a*b mod (X^N + 1, q), N = 65536, 868-bit q.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one product of the single-large-product workload (N = 65536, L = 28, seeded
+868-bit prime q, 99% uniform coefficients and 1% edge values). Prints one JSON line on rank 0.
+
+ours (default)
+  value        products/s with operands resident in HBM: per-step CUDA events on the
+               launching stream, L2 flushed (256 MiB write) before every timed step,
+               max over ranks (each rank runs its own products: weak scaling)
+  e2e          products/s through the reference-facing entry point fherma_run with host
+               buffers, timed by the library's harness runner exactly as the platform's harness
+               times it (steady clock around fherma_run: host copies, H2D, kernels, D2H)
+  roofline     dominant kernel's algorithmic IMAD rate against the IMAD peak measured live
+  cpu_baseline the CPU oracle (multi-prime NTT + CRT, OpenMP over all host cores) on one
+               product of the same workload (rank 0, N = 1 only)
+  batched      the same products back to back (device-resident, no flush between products)
+
+reference
+  the reference's own solution (solve.cu built unmodified for sm_100a except kMaxN raised to
+  65536, with its own generated harness main.cpp) on the same workload, timed by its harness;
+  falls back to the CPU oracle when that binary is absent or fails.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "engel-cuda-negacyclic-multiply_b200"
+sys.path.insert(0, str(PKG))
+
+METRIC = "products/s at N=2^16, 868-bit q, bit-exact: batched vs plain; serve p50/p99 ms"
+N_MAIN, BITS, SEED, EDGE = 65536, 868, 20261203, 0.01
+WORKLOAD = "single large product: N=65536, L=28, seeded 868-bit prime q, 1% edge coefficients"
+FLUSH_BYTES = 256 << 20
+RUNNER = PKG / "bin" / "solution"
+REF_BINARY = ROOT / "oracle" / "_ref" / "solution_n65536"
+TRAFFIC_FILE = ROOT / "profiles" / "traffic.json"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+    a.steps = max(a.steps, 1)
+    return a
+
+
+def config(parallelism: str) -> dict:
+    return {
+        "workload": WORKLOAD,
+        "N": N_MAIN,
+        "L": (BITS + 31) // 32,
+        "q_bits": BITS,
+        "edge_frac": EDGE,
+        "seed": SEED,
+        "l2": "flushed before every timed step (256 MiB device write)",
+        "parallelism": parallelism,
+    }
+
+
+# ----------------------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=self.file, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.file:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        load = [s for s in sm if smax and s > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- roofline
+
+
+def stage_work(k: int, N: int, L: int) -> list[float]:
+    """Algorithmic IMAD per stage: 8 per 64-bit mulmod, 2 per u32 x u64 limb MAC, 4 L per
+    coefficient for the final reduction. Whole product: 8 k N (1.5 log2 N + 7) + 6 k N L + 4 L N."""
+    logN = N.bit_length() - 1
+    logN2 = min(logN, 12)
+    logN1 = logN - logN2
+    mm1 = 2 * k * N + 2 * k * N + 2 * k * (N // 2) * logN1   # residue reductions, twists, column stages
+    mac1 = 2 * k * N * L
+    mm2 = 3 * k * (N // 2) * logN2 + k * N                    # three row transforms, pointwise
+    mm3 = k * (N // 2) * logN1 + k * N + k * N                # inverse column stages, untwist, CRT digit
+    mac3 = k * N * L
+    return [8 * mm1 + 2 * mac1, 8 * mm2, 8 * mm3 + 2 * mac3 + 4 * L * N]
+
+
+def stage_bytes(k: int, N: int, L: int) -> list[int]:
+    """Compulsory HBM bytes per stage (operands, residues, twiddles read once)."""
+    logN = N.bit_length() - 1
+    return [2 * N * L * 4 + 2 * k * N * 8,
+            2 * k * N * 8 + k * N * 8 + 2 * k * N * 16,
+            k * N * 8 + N * L * 4]
+
+
+# ----------------------------------------------------------------------------- harness runs
+
+
+def make_case_dir(root: Path, case, count: int) -> None:
+    import cases
+
+    cases.write_case_dir(root, case.N, case.W, case.L, case.q, [(case.a, case.b)])
+    src = root / "cases" / "000000"
+    for i in range(1, count):
+        d = root / "cases" / f"{i:06d}"
+        d.mkdir(parents=True, exist_ok=True)
+        for name in ("a.bin", "b.bin"):
+            os.link(src / name, d / name)
+    (root / "manifest.json").write_text(json.dumps({"N": case.N, "W": case.W, "L": case.L, "cases": count}))
+
+
+def run_harness(binary: Path, case, warmup: int, steps: int, timeout: float = 600.0):
+    """Run a harness binary over warmup + steps copies of one case; per-case seconds of the timed ones."""
+    import cases
+
+    with tempfile.TemporaryDirectory(prefix="nc_bench_") as tmp:
+        root = Path(tmp)
+        make_case_dir(root, case, warmup + steps)
+        r = subprocess.run([str(binary), str(root)], capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"{binary.name} exited {r.returncode}: {r.stderr[-400:]}")
+        res = cases.read_results(root)
+        rows = res["cases"]
+        if len(rows) != warmup + steps or any(row["status"] != "ok" for row in rows):
+            raise RuntimeError(f"{binary.name}: {sum(row['status'] != 'ok' for row in rows)} cases failed")
+        secs = [row["seconds"] for row in rows[warmup:]]
+        out = cases.read_output(root, warmup + steps - 1, case.N, case.L)
+        return secs, res["init_s"], out
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+
+
+def cpu_baseline(case, budget_s: float = 20.0) -> dict:
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    threads = oracle.max_threads()
+    times = []
+    t_all = time.perf_counter()
+    while not times or (time.perf_counter() - t_all < budget_s / 2 and len(times) < 3):
+        t0 = time.perf_counter()
+        oracle.negacyclic(case.N, case.q_limbs, case.a, case.b, threads)
+        times.append(time.perf_counter() - t0)
+    per = statistics.median(times)
+    return {"value": 1.0 / per, "unit": "products/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} product(s) of the N=65536 868-bit workload by the CPU oracle "
+                      f"(C, OpenMP over {threads} threads); median {per:.3f} s/product"}
+
+
+# ----------------------------------------------------------------------------- arms
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def ours(args) -> dict | None:
+    import numpy as np
+    import torch
+
+    import cases
+    import negacyclic as nc
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        pg = dist
+
+    case = cases.make_case(N_MAIN, BITS, SEED, edge_frac=EDGE)
+    plan = nc.Plan(case.N, case.q_limbs, W=case.W)
+    plan.set_timing(True)
+    n_pairs = 8  # distinct operand pairs: 8 x 22 MB of operands and outputs exceed L2
+    da = [torch.from_numpy(cases.coeffs(case.q, case.N, case.L, SEED + 10 * i + 1).view(np.int32)).to(dev)
+          for i in range(n_pairs)]
+    db = [torch.from_numpy(cases.coeffs(case.q, case.N, case.L, SEED + 10 * i + 2).view(np.int32)).to(dev)
+          for i in range(n_pairs)]
+    da[0].copy_(torch.from_numpy(case.a.view(np.int32)))
+    db[0].copy_(torch.from_numpy(case.b.view(np.int32)))
+    dc = [torch.empty_like(da[0]) for _ in range(n_pairs)]
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    def product(i):
+        j = i % n_pairs
+        plan.multiply_device(da[j].data_ptr(), db[j].data_ptr(), dc[j].data_ptr(), sh)
+
+    for i in range(args.warmup):
+        flush.zero_()
+        product(i)
+    torch.cuda.synchronize()
+    # correctness guard on the measured path: device result == host-entry result
+    ref = plan.multiply(case.a, case.b)
+    product(0)
+    torch.cuda.synchronize()
+    if not np.array_equal(dc[0].cpu().numpy().view(np.uint32), ref):
+        raise RuntimeError("device-resident product differs from the host entry point")
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stage = []
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev0[i].record(stream)
+            product(i)
+            ev1[i].record(stream)
+            torch.cuda.synchronize()
+            stage.append(plan.stage_ms())
+        # batched: the same products back to back, no flush between them
+        eb0 = torch.cuda.Event(enable_timing=True)
+        eb1 = torch.cuda.Event(enable_timing=True)
+        batch = 4 * n_pairs
+        plan.set_timing(False)
+        eb0.record(stream)
+        for i in range(batch):
+            product(i)
+        eb1.record(stream)
+        torch.cuda.synchronize()
+        plan.set_timing(True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
+    total_ms = sum(step_ms)
+    batch_ms = eb0.elapsed_time(eb1)
+    if pg:
+        t = torch.tensor([total_ms, batch_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms, batch_ms = float(t[0]), float(t[1])
+
+    peak = nc.imad_peak()
+    k, N, L = plan.k, case.N, case.L
+    mean_stage = [statistics.mean(s[i] for s in stage) for i in range(3)]
+    work = stage_work(k, N, L)
+    sbytes = stage_bytes(k, N, L)
+    dom = max(range(3), key=lambda i: mean_stage[i])
+    names = ["residues+forward columns", "row NTTs+pointwise", "inverse columns+CRT"]
+    kernels = ["k_dec", "k_row", "k_crt"]
+    traffic = None
+    if TRAFFIC_FILE.exists():
+        tf = json.loads(TRAFFIC_FILE.read_text())
+        traffic = tf.get(kernels[dom], {}).get("bytes_per_launch")
+    achieved = work[dom] / (mean_stage[dom] * 1e-3) / 1e9
+    result = {
+        "metric": METRIC,
+        "value": world * args.steps / (total_ms * 1e-3),
+        "unit": "products/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u64",
+        "data": "synthetic (seeded)",
+        "config": config(f"replicas{world}"),
+        "gpu_launches": 3 * args.steps,
+        "roofline": {
+            "bound": "imad",
+            "kernel": f"{kernels[dom]} ({names[dom]})",
+            "achieved": achieved,
+            "peak": peak / 1e9,
+            "unit": "GIMAD/s",
+            "frac": achieved * 1e9 / peak,
+            "traffic": traffic,
+            "peak_source": "measured live: mad.lo.u32 chains over every SM (nc_imad_peak)",
+            "stage_ms": mean_stage,
+            "stage_imad_alg": work,
+            "product_imad_alg": sum(work),
+            "product_frac": sum(work) / (total_ms / args.steps * 1e-3) / peak,
+            "stage_hbm_gbs": [b / (t * 1e-3) / 1e9 for b, t in zip(sbytes, mean_stage)],
+            "hbm_peak_gbs": _hbm_peak(),
+        },
+        "batched": {"products": batch, "value": world * batch / (batch_ms * 1e-3), "unit": "products/s",
+                    "form": "plain launches back to back, device-resident, 8 operand pairs rotated"},
+        "clocks": clk.summary(),
+    }
+    plan.close()
+
+    if rank == 0 and not args.no_e2e and RUNNER.exists():
+        secs, init_s, out = run_harness(RUNNER, case, args.warmup, args.steps)
+        if not np.array_equal(out, ref):
+            raise RuntimeError("harness runner output differs from the library")
+        per = statistics.mean(secs)
+        result["e2e"] = {"value": world / per, "unit": "products/s",
+                         "h2d_bytes_per_step": 2 * N * L * 4, "d2h_bytes_per_step": N * L * 4,
+                         "ms_p50": 1e3 * statistics.median(secs), "init_s": init_s,
+                         "via": "fherma_run in the library's harness runner (pageable std::vector in/out)"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(case)
+    if pg:
+        pg.destroy_process_group()
+    return result if rank == 0 else None
+
+
+def _hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return json.loads(p.read_text()).get("hbm_gbs")
+    except Exception:
+        return None
+
+
+def reference(args) -> dict | None:
+    import cases
+
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return None
+    case = cases.make_case(N_MAIN, BITS, SEED, edge_frac=EDGE)
+    base = {"metric": METRIC, "unit": "products/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64", "data": "synthetic (seeded)", "config": config("reference, one process")}
+    why = None
+    if REF_BINARY.exists():
+        try:
+            secs, init_s, _ = run_harness(REF_BINARY, case, args.warmup, args.steps)
+            per = statistics.mean(secs)
+            v = 1.0 / per
+            base.update({"value": v, "ms_per_step": 1e3 * per, "init_s": init_s,
+                         "cpu_baseline": {"value": v, "unit": "products/s", "cores": 1, "kind": "reference",
+                                          "sample": f"reference solve.cu (kMaxN raised to 65536, otherwise "
+                                                    f"unmodified, sm_100a) with its own harness main.cpp, "
+                                                    f"{args.steps} timed products after {args.warmup} warm-up; "
+                                                    f"its kernels run on the GPU, one host thread drives them"},
+                         "e2e": {"value": v, "unit": "products/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                         "gpu_launches": None})
+            return base
+        except Exception as e:  # fall back to the CPU oracle
+            why = str(e)[:300]
+    cb = cpu_baseline(case)
+    base.update({"value": cb["value"], "ms_per_step": 1e3 / cb["value"], "cpu_baseline": cb,
+                 "e2e": {"value": cb["value"], "unit": "products/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "note": f"reference binary unavailable ({why or 'not built'}); CPU oracle timed instead"})
+    return base
+
+
+def main() -> int:
+    args = parse_args()
+    out = reference(args) if args.impl == "reference" else ours(args)
+    if out is not None:
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
