@@ -244,6 +244,7 @@ def ours(args) -> dict | None:
 
     case = cases.make_case(N_MAIN, BITS, SEED, edge_frac=EDGE)
     plan = nc.Plan(case.N, case.q_limbs, W=case.W)
+    tuned_ms = plan.autotune(reps=3)  # untimed: picks the row tiling for N = 65536
     plan.set_timing(True)
     n_pairs = 8  # distinct operand pairs: 8 x 22 MB of operands and outputs exceed L2
     da = [torch.from_numpy(cases.coeffs(case.q, case.N, case.L, SEED + 10 * i + 1).view(np.int32)).to(dev)
@@ -336,6 +337,8 @@ def ours(args) -> dict | None:
         "data": "synthetic (seeded)",
         "config": config(f"replicas{world}"),
         "gpu_launches": 3 * args.steps,
+        "row_config": {"log_block": plan.row_config[0], "log_radix": plan.row_config[1],
+                       "threads": plan.row_config[2], "autotune_ms": tuned_ms},
         "roofline": {
             "bound": "imad",
             "kernel": f"{kernels[dom]} ({names[dom]})",

@@ -3,9 +3,11 @@
 #include "fherma.h"
 #include "negacyclic_b200.h"
 
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
+#include "batch.h"
 #include "engine.h"
 #include "hostmath.h"
 #include "kernels.h"
@@ -132,7 +134,18 @@ int nc_primes(uint64_t* out, int count) {
 void* fherma_init(const fherma::Point& point) {
     if (point.q.data.size() != point.L) throw std::runtime_error("q must hold L limbs");
     try {
-        return nc::plan_create(point.N, point.W, point.L, point.q.data.data());
+        nc::Plan* p = nc::plan_create(point.N, point.W, point.L, point.q.data.data());
+        // init is not timed by the harness: pick the row tiling for this N on the device now
+        const char* tune = std::getenv("NC_AUTOTUNE");
+        if (!(tune && tune[0] == '0')) {
+            try {
+                nc::plan_autotune(p, 3);
+            } catch (...) {
+                nc::plan_destroy(p);
+                throw;
+            }
+        }
+        return p;
     } catch (const nc::Error& e) {
         throw std::runtime_error(e.what());
     }
@@ -146,9 +159,10 @@ fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
         throw std::runtime_error("a and b must contain N*L limbs");
     fherma::Outputs out;
     out.c.shape = {int64_t(p->N), int64_t(p->L)};
-    out.c.data.resize(count);
     try {
-        nc::plan_multiply_host(p, in.a.data.data(), in.b.data.data(), out.c.data.data());
+        nc::plan_submit_host(p, in.a.data.data(), in.b.data.data());
+        out.c.data.resize(count);  // zero-fills on the host while the GPU computes
+        nc::plan_collect_host(p, out.c.data.data());
     } catch (const nc::Error& e) {
         throw std::runtime_error(e.what());
     }
@@ -156,3 +170,126 @@ fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
 }
 
 void fherma_free(void* state) { nc::plan_destroy(static_cast<nc::Plan*>(state)); }
+
+// ------------------------------------------------------------------ tuning and batches
+
+struct nc_batch {
+    nc::Batch* b;
+};
+
+extern "C" {
+
+int nc_row_variants(uint32_t log_n, int* triples, int max_variants) {
+    if (log_n < 1 || log_n > uint32_t(nc::kMaxLogN) || (!triples && max_variants > 0)) {
+        g_last_error = "log_n must be 1..16";
+        return NC_EINVAL;
+    }
+    const auto v = nc::row_variants(int(log_n));
+    int n = 0;
+    for (const auto& c : v) {
+        if (n >= max_variants) break;
+        triples[3 * n] = c.logN2;
+        triples[3 * n + 1] = c.logE;
+        triples[3 * n + 2] = c.threads;
+        ++n;
+    }
+    return max_variants <= 0 ? int(v.size()) : n;
+}
+
+int nc_plan_set_row_config(nc_plan* plan, int log_block, int log_radix, int threads) {
+    return guarded([&] {
+        if (!plan) throw nc::Error(nc::kEInval, "null plan");
+        nc::plan_set_row_config(plan->p, nc::RowConfig{log_block, log_radix, threads});
+    });
+}
+
+int nc_plan_get_row_config(const nc_plan* plan, int* log_block, int* log_radix, int* threads) {
+    return guarded([&] {
+        if (!plan) throw nc::Error(nc::kEInval, "null plan");
+        if (log_block) *log_block = plan->p->cfg.logN2;
+        if (log_radix) *log_radix = plan->p->cfg.logE;
+        if (threads) *threads = plan->p->cfg.threads;
+    });
+}
+
+int nc_plan_autotune(nc_plan* plan, int reps, float* best_ms) {
+    return guarded([&] {
+        if (!plan) throw nc::Error(nc::kEInval, "null plan");
+        const float ms = nc::plan_autotune(plan->p, reps);
+        if (best_ms) *best_ms = ms;
+    });
+}
+
+uint64_t nc_plan_hat_words(const nc_plan* plan) {
+    return plan ? uint64_t(plan->p->k) * uint64_t(plan->p->N) : 0;
+}
+
+int nc_batch_create(nc_batch** out) {
+    return guarded([&] {
+        if (!out) throw nc::Error(nc::kEInval, "out is null");
+        *out = nullptr;
+        auto* b = new nc::Batch(nc::current_device());
+        *out = new nc_batch{b};
+    });
+}
+
+int nc_batch_destroy(nc_batch* batch) {
+    return guarded([&] {
+        if (!batch) return;
+        delete batch->b;
+        delete batch;
+    });
+}
+
+int nc_batch_add(nc_batch* batch, nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c) {
+    return guarded([&] {
+        if (!batch || !plan) throw nc::Error(nc::kEInval, "null batch or plan");
+        batch->b->add(plan->p, nc::kModeProduct, d_a, d_b, d_c, nullptr, nullptr);
+    });
+}
+
+int nc_batch_add_cached(nc_batch* batch, nc_plan* plan, const uint64_t* d_a_hat, const uint32_t* d_b, uint32_t* d_c) {
+    return guarded([&] {
+        if (!batch || !plan) throw nc::Error(nc::kEInval, "null batch or plan");
+        batch->b->add(plan->p, nc::kModeCachedA, nullptr, d_b, d_c, d_a_hat, nullptr);
+    });
+}
+
+int nc_batch_add_forward(nc_batch* batch, nc_plan* plan, const uint32_t* d_a, uint64_t* d_a_hat) {
+    return guarded([&] {
+        if (!batch || !plan) throw nc::Error(nc::kEInval, "null batch or plan");
+        batch->b->add(plan->p, nc::kModeForward, d_a, nullptr, nullptr, nullptr, d_a_hat);
+    });
+}
+
+int nc_batch_clear(nc_batch* batch) {
+    return guarded([&] {
+        if (!batch) throw nc::Error(nc::kEInval, "null batch");
+        batch->b->clear();
+    });
+}
+
+int nc_batch_run(nc_batch* batch, void* stream, int use_graph) {
+    return guarded([&] {
+        if (!batch) throw nc::Error(nc::kEInval, "null batch");
+        batch->b->run(static_cast<cudaStream_t>(stream), use_graph != 0);
+    });
+}
+
+int nc_batch_synchronize(nc_batch* batch) {
+    return guarded([&] {
+        if (!batch) throw nc::Error(nc::kEInval, "null batch");
+        batch->b->synchronize();
+    });
+}
+
+int nc_batch_query(const nc_batch* batch, uint32_t* products, uint32_t* ctas, uint64_t* scratch_bytes) {
+    return guarded([&] {
+        if (!batch) throw nc::Error(nc::kEInval, "null batch");
+        if (products) *products = uint32_t(batch->b->size());
+        if (ctas) *ctas = uint32_t(batch->b->ctas());
+        if (scratch_bytes) *scratch_bytes = uint64_t(batch->b->scratch_bytes());
+    });
+}
+
+}  // extern "C"

@@ -60,6 +60,15 @@ __device__ __forceinline__ uint64_t reduce_special(uint64_t hi, uint64_t lo, uin
     return static_cast<uint64_t>(static_cast<uint32_t>(h2)) * m0 + (t_lo & kMask62);  // < 2^62 + 2^59
 }
 
+// S = (a2:a1:a0) + (b2:b1:b0) * 2^32 (< 2^99, a limb-by-constant sum) reduced mod p into [0, 2p).
+__device__ __forceinline__ uint64_t reduce_limb_sum(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t b0, uint32_t b1,
+                                                    uint32_t b2, uint64_t m) {
+    const uint64_t lo_a = (uint64_t(a1) << 32) | a0;
+    const uint64_t lo = lo_a + (uint64_t(b0) << 32);
+    const uint64_t hi = uint64_t(a2) + b1 + (uint64_t(b2) << 32) + (lo < lo_a ? 1u : 0u);
+    return reduce_special(hi, lo, m);
+}
+
 // y * z mod p in [0, 2p) for y < 2^62 and z < 2^64 (pointwise product of two transforms).
 __device__ __forceinline__ uint64_t mulmod_special(uint64_t y, uint64_t z, uint64_t m) {
     return reduce_special(__umul64hi(y, z), y * z, m);

@@ -1,0 +1,186 @@
+// Batches of products run by one persistent kernel launch (host side; see batch.h).
+#include "batch.h"
+
+#include <algorithm>
+#include <cstring>
+
+#include "batch_types.h"
+#include "kernel_registry.h"
+#include "kernels.h"
+
+namespace nc {
+
+namespace {
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+template <class T>
+void ensure(T** p, size_t* cap, size_t count, const char* what) {
+    if (count <= *cap && *p) return;
+    cudaFree(*p);
+    *p = nullptr;
+    const size_t n = std::max<size_t>(count, 1) * 2;
+    check(cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T)), what);
+    *cap = n;
+}
+
+}  // namespace
+
+Batch::Batch(int device) : device_(device) { tables_ = acquire_tables(device); }
+
+Batch::~Batch() {
+    if (last_stream_) cudaStreamSynchronize(last_stream_);
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    cudaFree(d_products_);
+    cudaFree(d_items_);
+    cudaFree(d_state_);
+    cudaFree(scratch_);
+    release_tables(tables_);
+}
+
+void Batch::add(Plan* plan, uint32_t mode, const uint32_t* a, const uint32_t* b, uint32_t* c, const uint64_t* a_hat,
+                uint64_t* hat_out) {
+    if (!plan) throw Error(kEInval, "null plan");
+    if (plan->device != device_) throw Error(kEInval, "the plan lives on another device");
+    if (mode > kModeForward) throw Error(kEInval, "unknown product mode");
+    const bool need_a = mode != kModeCachedA, need_b = mode != kModeForward;
+    if ((need_a && !a) || (need_b && (!b || !c)) || (mode == kModeCachedA && !a_hat) ||
+        (mode == kModeForward && !hat_out))
+        throw Error(kEInval, "missing device buffer for this product mode");
+    const uintptr_t align = reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) |
+                            reinterpret_cast<uintptr_t>(c) | reinterpret_cast<uintptr_t>(a_hat) |
+                            reinterpret_cast<uintptr_t>(hat_out);
+    if (align & 15) throw Error(kEInval, "device buffers must be 16-byte aligned");
+    if (entries_.size() >= (size_t(1) << 28)) throw Error(kEInval, "batch too large");
+    entries_.push_back(Entry{plan, mode, a, b, c, a_hat, hat_out});
+    dirty_ = true;
+}
+
+void Batch::clear() {
+    entries_.clear();
+    dirty_ = true;
+}
+
+void Batch::finalize() {
+    const size_t n = entries_.size();
+    std::vector<BatchProduct> prods(n);
+    std::vector<uint64_t> shape;
+    size_t scratch = 0;
+    int kmax = 1;
+    for (size_t p = 0; p < n; ++p) {
+        const Plan* pl = entries_[p].plan;
+        scratch += 2 * round_up(size_t(pl->k) * pl->N * sizeof(uint64_t), 256);
+        kmax = std::max(kmax, pl->k);
+    }
+    if (scratch > scratch_bytes_) {
+        cudaFree(scratch_);
+        scratch_ = nullptr;
+        scratch_bytes_ = 0;
+        check(cudaMalloc(&scratch_, scratch), "batch scratch");
+        scratch_bytes_ = scratch;
+    }
+    std::vector<uint2> dec, row, crt;
+    size_t off = 0;
+    char* base = reinterpret_cast<char*>(scratch_);
+    for (size_t p = 0; p < n; ++p) {
+        const Entry& e = entries_[p];
+        const Plan* pl = e.plan;
+        const RowConfig cfg = default_row_config(pl->logN);
+        const Geometry g = geometry(pl->logN, pl->k, cfg);
+        ProductDesc d = pl->desc(e.a, e.b, e.c);
+        d.logN2 = uint32_t(cfg.logN2);
+        d.mode = e.mode;
+        d.a_hat = e.a_hat;
+        d.hat_out = e.hat_out;
+        const size_t res = round_up(size_t(pl->k) * pl->N * sizeof(uint64_t), 256);
+        d.ra = reinterpret_cast<uint64_t*>(base + off);
+        d.rb = reinterpret_cast<uint64_t*>(base + off + res);
+        off += 2 * res;
+        BatchProduct& bp = prods[p];
+        bp.d = d;
+        bp.tiles = uint32_t(g.tiles);
+        bp.first_operand = e.mode == kModeCachedA ? 1u : 0u;
+        bp.n_dec = uint32_t((e.mode == kModeProduct ? 2 : 1) * g.tiles);
+        bp.n_row = uint32_t(g.row_ctas);
+        const uint32_t pid = uint32_t(p);
+        for (uint32_t i = 0; i < bp.n_dec; ++i) dec.push_back(make_uint2((kItemDec << 28) | pid, i));
+        for (uint32_t i = 0; i < bp.n_row; ++i) row.push_back(make_uint2((kItemRow << 28) | pid, i));
+        if (e.mode != kModeForward)
+            for (uint32_t i = 0; i < uint32_t(g.tiles); ++i) crt.push_back(make_uint2((kItemCrt << 28) | pid, i));
+        shape.push_back((uint64_t(pl->logN) << 40) | (uint64_t(pl->k) << 32) | (uint64_t(pl->L) << 8) | e.mode);
+    }
+    std::vector<uint2> items;
+    items.reserve(dec.size() + row.size() + crt.size());
+    items.insert(items.end(), dec.begin(), dec.end());
+    items.insert(items.end(), row.begin(), row.end());
+    items.insert(items.end(), crt.begin(), crt.end());
+    n_items_ = int(items.size());
+
+    ensure(reinterpret_cast<char**>(&d_products_), &products_cap_, n * sizeof(BatchProduct), "batch products");
+    ensure(&d_items_, &items_cap_, items.size(), "batch items");
+    ensure(&d_state_, &state_cap_, 2 * n + 2, "batch counters");
+    if (n) check(cudaMemcpy(d_products_, prods.data(), n * sizeof(BatchProduct), cudaMemcpyHostToDevice), "upload");
+    if (!items.empty())
+        check(cudaMemcpy(d_items_, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice), "upload");
+
+    smem_ = smax(smax(dec_smem_bytes(kmax), crt_smem_bytes(kmax)), row_smem_bytes(kThreads, 4));
+    int per_sm = 0, sms = 0;
+    check(persistent_occupancy(smem_, &per_sm), "occupancy");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "device attribute");
+    ctas_ = std::max(1, std::min(per_sm * sms, n_items_));
+    if (shape != shape_) {
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        exec_ = nullptr;
+        graph_ = nullptr;
+        shape_ = shape;
+    }
+    dirty_ = false;
+}
+
+void Batch::run(cudaStream_t stream, bool use_graph) {
+    if (entries_.empty()) return;
+    if (dirty_) finalize();
+    const size_t n = entries_.size();
+    BatchArgs args{};
+    args.products = static_cast<const BatchProduct*>(d_products_);
+    args.items = d_items_;
+    args.n_items = n_items_;
+    args.counters = d_state_;
+    args.head = d_state_ + 2 * n;
+    args.error = d_state_ + 2 * n + 1;
+    args.tables = tables_->view();
+    const size_t state_bytes = (2 * n + 2) * sizeof(uint32_t);
+    last_stream_ = stream;
+    if (!use_graph) {
+        check(cudaMemsetAsync(d_state_, 0, state_bytes, stream), "batch reset");
+        check(launch_persistent(args, ctas_, smem_, stream), "persistent launch");
+        return;
+    }
+    if (!exec_) {
+        cudaStream_t cap = nullptr;
+        check(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "capture stream");
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaMemsetAsync(d_state_, 0, state_bytes, cap);
+            launch_persistent(args, ctas_, smem_, cap);
+            e = cudaStreamEndCapture(cap, &graph_);
+        }
+        cudaStreamDestroy(cap);
+        check(e, "graph capture");
+        check(cudaGraphInstantiate(&exec_, graph_, 0), "graph instantiate");
+    }
+    check(cudaGraphLaunch(exec_, stream), "graph launch");
+}
+
+void Batch::synchronize() {
+    if (!last_stream_ && entries_.empty()) return;
+    check(cudaStreamSynchronize(last_stream_), "batch");
+    if (entries_.empty()) return;
+    uint32_t err = 0;
+    check(cudaMemcpy(&err, d_state_ + 2 * entries_.size() + 1, sizeof(err), cudaMemcpyDeviceToHost), "batch status");
+    if (err) throw Error(kETimeout, "a persistent-kernel dependency wait gave up");
+}
+
+}  // namespace nc

@@ -1,0 +1,69 @@
+// Batches of products run by one persistent kernel launch (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "engine.h"
+
+namespace nc {
+
+
+// A list of products (each referring to a plan for its q, N and constants) that run together.
+// Products may differ in N and in q. Residue scratch comes from the batch's own arena; the
+// counter reset and the launch are captured once into a CUDA graph and replayed while the
+// batch keeps the same shape.
+class Batch {
+  public:
+    explicit Batch(int device);
+    ~Batch();
+
+    // mode: kModeProduct (a, b -> c), kModeCachedA (a_hat in the NTT domain, b -> c),
+    //       kModeForward (a -> a_hat: the NTT-domain form of an operand, for caching).
+    void add(Plan* plan, uint32_t mode, const uint32_t* a, const uint32_t* b, uint32_t* c, const uint64_t* a_hat,
+             uint64_t* hat_out);
+    void clear();
+    size_t size() const { return entries_.size(); }
+    // Enqueue the whole batch on `stream` (graph replay when `use_graph`).
+    void run(cudaStream_t stream, bool use_graph);
+    // Wait for the last run and check that no dependency wait gave up.
+    void synchronize();
+    int ctas() const { return ctas_; }
+    size_t scratch_bytes() const { return scratch_bytes_; }
+    int launches_per_run() const { return 1; }
+
+  private:
+    struct Entry {
+        Plan* plan;
+        uint32_t mode;
+        const uint32_t* a;
+        const uint32_t* b;
+        uint32_t* c;
+        const uint64_t* a_hat;
+        uint64_t* hat_out;
+    };
+    void finalize();
+    int device_;
+    std::vector<Entry> entries_;
+    std::vector<uint64_t> shape_;  // signature of the captured graph
+    DeviceTables* tables_ = nullptr;
+    void* d_products_ = nullptr;
+    size_t products_cap_ = 0;
+    uint2* d_items_ = nullptr;
+    size_t items_cap_ = 0;
+    uint32_t* d_state_ = nullptr;  // counters (2 per product), head, error
+    size_t state_cap_ = 0;
+    uint64_t* scratch_ = nullptr;
+    size_t scratch_bytes_ = 0;
+    int n_items_ = 0;
+    int ctas_ = 0;
+    size_t smem_ = 0;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    cudaStream_t last_stream_ = nullptr;
+    bool dirty_ = true;
+};
+
+}  // namespace nc

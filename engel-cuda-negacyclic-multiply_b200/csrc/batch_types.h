@@ -1,0 +1,33 @@
+// Plain-old-data shared by the persistent kernel and its host side.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.h"
+
+namespace nc {
+
+enum : uint32_t { kItemDec = 0, kItemRow = 1, kItemCrt = 2 };
+
+// One product of a batch with the item counts its dependents wait for.
+struct BatchProduct {
+    ProductDesc d;
+    uint32_t n_dec;          // residue items of this product
+    uint32_t n_row;          // row items
+    uint32_t tiles;          // residue tiles per operand
+    uint32_t first_operand;  // 1 when a is given in the NTT domain (only b is decomposed)
+};
+
+struct BatchArgs {
+    const BatchProduct* products;
+    const uint2* items;  // x = stage << 28 | product, y = index inside the stage
+    int n_items;
+    uint32_t* counters;  // per product: residue items done, row items done
+    uint32_t* head;      // next queue position
+    uint32_t* error;     // nonzero once a wait gave up
+    Tables tables;
+};
+
+}  // namespace nc

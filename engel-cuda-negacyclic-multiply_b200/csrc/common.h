@@ -7,8 +7,16 @@
 // same canonical output, so this build fixes the set once.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <cstdint>
+
+#ifdef __CUDACC__
+#define NC_HD __host__ __device__
+#else
+#define NC_HD
+#endif
 
 namespace nc {
 
@@ -64,33 +72,83 @@ struct ProductDesc {
     uint32_t LW;
     uint32_t k;
     uint32_t mode;          // kModeProduct, kModeCachedA, kModeForward
-    uint32_t pad;
+    uint32_t logN2;         // row block size of the row configuration (N1 = N >> logN2)
 };
 
 enum : uint32_t { kModeProduct = 0, kModeCachedA = 1, kModeForward = 2 };
 
-// Geometry of one product: row blocks of N2 = 2^logN2 residues and a column transform of
-// N1 = 2^logN1 points over them (N = N1 * N2).
+// Device-wide twiddle tables (built once per device). Entry j of prime i sits at
+// fwd[i * kMaxN + j] = psi^bitrev16(j) with its Shoup companion (inv: psi^-bitrev16(j)); the
+// first N entries are the merged twiddles of every ring degree N <= 2^16.
+struct Tables {
+    const ulonglong2* fwd;    // [kMaxPrimes][kMaxN]
+    const ulonglong2* inv;    // [kMaxPrimes][kMaxN]
+};
+
+// Dynamic shared memory of each stage.
+NC_HD constexpr size_t smax(size_t a, size_t b) { return a > b ? a : b; }
+NC_HD constexpr size_t dec_smem_bytes(int k) { return smax(size_t(kTile) * kMaxL * 4, size_t(kTile) * 8 * size_t(k)); }
+NC_HD constexpr size_t row_smem_bytes(int threads, int logE) { return size_t(2) * size_t(threads) * (size_t(1) << logE) * 8; }
+NC_HD constexpr size_t crt_smem_bytes(int k) {
+    return smax(size_t(kTile) * 8 * size_t(k), size_t(kTile) * kMaxL * 4)  // residues / output staging
+           + size_t(k) * kMqStride * 4                                       // M/p_i mod q
+           + size_t(k) * 8 * 2                                               // y, y shoup
+           + size_t(kMqStride) * 4 * 2 + 16;                                 // -M mod q, q, mu
+}
+
+// How the row stage tiles a product: row blocks of N2 = 2^logN2 residues, each thread holding
+// 2^logE of them per register pass (the NTT radix), CTAs of `threads` threads. The column
+// transform then has N1 = N / N2 points (at most 32).
+struct RowConfig {
+    int logN2;
+    int logE;
+    int threads;
+};
+
+constexpr int kMaxLogN1 = 5;
+constexpr int kRowLogCap = 13;
+
+inline RowConfig default_row_config(int logN) {
+    RowConfig c{};
+    c.logN2 = logN < kRowLogMax ? logN : kRowLogMax;
+    c.logE = 4;
+    c.threads = 256;
+    return c;
+}
+
+// Geometry of one product under a row configuration.
 struct Geometry {
-    int logN, logN1, logN2;
+    int logN, logN1, logN2, logE, row_threads;
     int tile;             // coefficients per decomposition / CRT tile
     int tiles;            // tiles per operand
-    int rows_per_cta;     // row blocks per row-stage CTA (> 1 only when N2 < 4096)
+    int rows_per_cta;     // row blocks per row-stage CTA
     int row_ctas;         // CTAs of the row stage
 };
 
-inline Geometry geometry(int logN, int k) {
+inline bool row_config_valid(int logN, const RowConfig& c) {
+    if (c.logN2 < 1 || c.logN2 > kRowLogCap || c.logN2 > logN) return false;
+    if (logN - c.logN2 > kMaxLogN1) return false;
+    if (logN > kRowLogMax && c.logN2 < logN - kMaxLogN1) return false;
+    if (c.logE != 3 && c.logE != 4) return false;
+    if (c.threads != 256 && c.threads != 512) return false;
+    const int le = c.logE < c.logN2 ? c.logE : c.logN2;
+    const int t = 1 << (c.logN2 - le);
+    return t <= c.threads;
+}
+
+inline Geometry geometry(int logN, int k, const RowConfig& c) {
     Geometry g{};
     g.logN = logN;
-    g.logN2 = logN < kRowLogMax ? logN : kRowLogMax;
-    g.logN1 = logN - g.logN2;
+    g.logN2 = c.logN2;
+    g.logN1 = logN - c.logN2;
+    g.logE = c.logE;
+    g.row_threads = c.threads;
     const int n = 1 << logN;
     g.tile = n < kTile ? n : kTile;
     g.tiles = n / g.tile;
-    const int n2 = 1 << g.logN2;
-    const int e = n2 >= 16 ? 16 : n2;
-    const int threads_per_row = n2 / e;
-    g.rows_per_cta = kThreads / threads_per_row;
+    const int le = c.logE < c.logN2 ? c.logE : c.logN2;
+    const int threads_per_row = 1 << (c.logN2 - le);
+    g.rows_per_cta = c.threads / threads_per_row;
     const int blocks = k << g.logN1;
     g.row_ctas = (blocks + g.rows_per_cta - 1) / g.rows_per_cta;
     return g;

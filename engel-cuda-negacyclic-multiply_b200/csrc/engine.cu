@@ -1,6 +1,8 @@
 // Plans, device tables and the host-buffer pipeline (see engine.h).
 #include "engine.h"
 
+#include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -46,20 +48,12 @@ DeviceTables* acquire_tables(int device) {
         const size_t tw_bytes = size_t(kMaxPrimes) * kMaxN * sizeof(ulonglong2);
         check(cudaMalloc(&t->fwd, tw_bytes), "twiddle table");
         check(cudaMalloc(&t->inv, tw_bytes), "inverse twiddle table");
-        check(cudaMalloc(&t->pow32, h.pow32.size() * sizeof(uint64_t)), "residue places");
-        check(cudaMalloc(&t->pc, h.pc.size() * sizeof(PrimeConst)), "prime constants");
         check(cudaMemcpy(t->fwd, h.fwd.data(), tw_bytes, cudaMemcpyHostToDevice), "twiddle upload");
         check(cudaMemcpy(t->inv, h.inv.data(), tw_bytes, cudaMemcpyHostToDevice), "inverse twiddle upload");
-        check(cudaMemcpy(t->pow32, h.pow32.data(), h.pow32.size() * sizeof(uint64_t), cudaMemcpyHostToDevice),
-              "residue places upload");
-        check(cudaMemcpy(t->pc, h.pc.data(), h.pc.size() * sizeof(PrimeConst), cudaMemcpyHostToDevice),
-              "prime constants upload");
-        check(prepare_plain_kernels(), "kernel attributes");
+        check(prepare_kernels(h.pc.data(), h.pow32.data()), "kernel preparation");
     } catch (...) {
         cudaFree(t->fwd);
         cudaFree(t->inv);
-        cudaFree(t->pow32);
-        cudaFree(t->pc);
         delete t;
         throw;
     }
@@ -78,67 +72,59 @@ void release_tables(DeviceTables* t) {
     cudaSetDevice(t->device);
     cudaFree(t->fwd);
     cudaFree(t->inv);
-    cudaFree(t->pow32);
-    cudaFree(t->pc);
     cudaSetDevice(prev);
     delete t;
 }
 
-// ------------------------------------------------------------------------------ host copies
+// ------------------------------------------------------------------------------ host pool
 
-ParallelCopy::ParallelCopy(int threads) {
-    for (int w = 1; w < threads; ++w)
-        workers_.emplace_back([this, w] {
-            uint64_t seen = 0;
-            for (;;) {
-                {
-                    std::unique_lock<std::mutex> lock(mu_);
-                    cv_.wait(lock, [&] { return stop_ || gen_ != seen; });
-                    if (stop_) return;
-                    seen = gen_;
-                }
-                run_part(w);
-                std::lock_guard<std::mutex> lock(mu_);
-                if (--pending_ == 0) done_cv_.notify_all();
-            }
-        });
+HostPool::HostPool(int threads) {
+    for (int w = 1; w < threads; ++w) workers_.emplace_back([this, w] { worker(w); });
 }
 
-ParallelCopy::~ParallelCopy() {
+HostPool::~HostPool() {
     {
         std::lock_guard<std::mutex> lock(mu_);
-        stop_ = true;
+        stop_.store(true);
     }
     cv_.notify_all();
     for (auto& w : workers_) w.join();
 }
 
-void ParallelCopy::run_part(int part) {
-    const size_t parts = workers_.size() + 1;
-    const size_t chunk = ((bytes_ + parts - 1) / parts + 63) & ~size_t(63);
-    const size_t begin = chunk * size_t(part);
-    if (begin >= bytes_) return;
-    const size_t n = (begin + chunk > bytes_) ? bytes_ - begin : chunk;
-    std::memcpy(dst_ + begin, src_ + begin, n);
+void HostPool::worker(int part) {
+    uint64_t seen = 0;
+    for (;;) {
+        // spin for a short while (jobs of one product come back to back), then sleep
+        const auto spin_until = std::chrono::steady_clock::now() + std::chrono::microseconds(300);
+        while (gen_.load(std::memory_order_acquire) == seen && !stop_.load() &&
+               std::chrono::steady_clock::now() < spin_until) {
+        }
+        if (gen_.load(std::memory_order_acquire) == seen && !stop_.load()) {
+            std::unique_lock<std::mutex> lock(mu_);
+            cv_.wait(lock, [&] { return stop_.load() || gen_.load() != seen; });
+        }
+        if (stop_.load()) return;
+        seen = gen_.load(std::memory_order_acquire);
+        (*job_)(part, parts());
+        pending_.fetch_sub(1, std::memory_order_acq_rel);
+    }
 }
 
-void ParallelCopy::copy(void* dst, const void* src, size_t bytes) {
-    if (workers_.empty() || bytes < (size_t(1) << 20)) {
-        std::memcpy(dst, src, bytes);
+void HostPool::run(const std::function<void(int, int)>& fn) {
+    if (workers_.empty()) {
+        fn(0, 1);
         return;
     }
+    job_ = &fn;
+    pending_.store(int(workers_.size()), std::memory_order_relaxed);
     {
         std::lock_guard<std::mutex> lock(mu_);
-        dst_ = static_cast<char*>(dst);
-        src_ = static_cast<const char*>(src);
-        bytes_ = bytes;
-        pending_ = int(workers_.size());
-        ++gen_;
+        gen_.fetch_add(1, std::memory_order_acq_rel);
     }
     cv_.notify_all();
-    run_part(0);
-    std::unique_lock<std::mutex> lock(mu_);
-    done_cv_.wait(lock, [&] { return pending_ == 0; });
+    fn(0, parts());
+    while (pending_.load(std::memory_order_acquire) != 0) {
+    }
 }
 
 // ------------------------------------------------------------------------------ plans
@@ -156,6 +142,7 @@ ProductDesc Plan::desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const 
     d.LW = hq.LW;
     d.k = uint32_t(k);
     d.mode = kModeProduct;
+    d.logN2 = uint32_t(cfg.logN2);
     return d;
 }
 
@@ -190,6 +177,7 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
         throw Error(kEInval, "W must be the bit width of q and L = (W + 31) / 32");
     }
     p->k = int(p->hq.k);
+    if (!tuned_row_config(logN, int(L), &p->cfg)) p->cfg = default_row_config(logN);
     try {
         p->device = current_device();
         p->tables = acquire_tables(p->device);
@@ -209,7 +197,9 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
         check(cudaEventCreate(&p->ev_start), "event");
         check(cudaEventCreate(&p->ev_stop), "event");
         for (auto& ev : p->ev_stage) check(cudaEventCreate(&ev), "event");
-        p->copier = new ParallelCopy(copy_threads());
+        p->pool = new HostPool(copy_threads());
+        p->ev_out.assign(size_t(p->pool->parts()), nullptr);
+        for (auto& ev : p->ev_out) check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
     } catch (...) {
         plan_destroy(p);
         throw;
@@ -234,7 +224,9 @@ void plan_destroy(Plan* p) {
     for (auto ev : p->ev_stage)
         if (ev) cudaEventDestroy(ev);
     if (p->stream) cudaStreamDestroy(p->stream);
-    delete p->copier;
+    for (auto ev : p->ev_out)
+        if (ev) cudaEventDestroy(ev);
+    delete p->pool;
     release_tables(p->tables);
     delete p;
 }
@@ -246,26 +238,150 @@ void plan_multiply_device(Plan* p, const uint32_t* d_a, const uint32_t* d_b, uin
          15) != 0)
         throw Error(kEInval, "device buffers must be 16-byte aligned");
     const ProductDesc d = p->desc(d_a, d_b, d_c);
-    check(launch_product(d, p->tables->view(), stream, p->timing ? p->ev_stage : nullptr), "kernel launch");
+    check(launch_product(d, p->tables->view(), p->cfg, stream, p->timing ? p->ev_stage : nullptr),
+          "kernel launch");
 }
 
-void plan_multiply_host(Plan* p, const uint32_t* a, const uint32_t* b, uint32_t* c) {
+namespace {
+
+// [lo, hi) of part `part` out of `parts` for `bytes`, in 4 KiB granules.
+void slice(size_t bytes, int part, int parts, size_t* lo, size_t* hi) {
+    const size_t granules = (bytes + 4095) / 4096;
+    const size_t per = (granules + size_t(parts) - 1) / size_t(parts);
+    *lo = std::min(bytes, per * size_t(part) * 4096);
+    *hi = std::min(bytes, per * size_t(part + 1) * 4096);
+}
+
+constexpr size_t kSubChunk = size_t(256) << 10;  // staging granule: memcpy, then enqueue its DMA
+
+}  // namespace
+
+void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
     if (!p) throw Error(kEInval, "null plan");
-    if (!a || !b || !c) throw Error(kEInval, "null host buffer");
+    if (!a || !b) throw Error(kEInval, "null host buffer");
     const size_t bytes = p->limbs() * sizeof(uint32_t);
-    p->copier->copy(p->h_a, a, bytes);
-    check(cudaMemcpyAsync(p->d_a, p->h_a, bytes, cudaMemcpyHostToDevice, p->stream), "a copy");
-    p->copier->copy(p->h_b, b, bytes);
-    check(cudaMemcpyAsync(p->d_b, p->h_b, bytes, cudaMemcpyHostToDevice, p->stream), "b copy");
+    std::atomic<int> err{int(cudaSuccess)};
+    p->pool->run([&](int part, int parts) {
+        size_t lo, hi;
+        slice(bytes, part, parts, &lo, &hi);
+        const char* srcs[2] = {reinterpret_cast<const char*>(a), reinterpret_cast<const char*>(b)};
+        char* pins[2] = {reinterpret_cast<char*>(p->h_a), reinterpret_cast<char*>(p->h_b)};
+        char* devs[2] = {reinterpret_cast<char*>(p->d_a), reinterpret_cast<char*>(p->d_b)};
+        for (int op = 0; op < 2; ++op)
+            for (size_t off = lo; off < hi; off += kSubChunk) {
+                const size_t n = std::min(kSubChunk, hi - off);
+                std::memcpy(pins[op] + off, srcs[op] + off, n);
+                const cudaError_t e = cudaMemcpyAsync(devs[op] + off, pins[op] + off, n, cudaMemcpyHostToDevice,
+                                                      p->stream);
+                if (e != cudaSuccess) err.store(int(e));
+            }
+    });
+    check(cudaError_t(err.load()), "operand copy");
     check(cudaEventRecord(p->ev_start, p->stream), "event");
-    check(launch_product(p->desc(p->d_a, p->d_b, p->d_c), p->tables->view(), p->stream,
+    check(launch_product(p->desc(p->d_a, p->d_b, p->d_c), p->tables->view(), p->cfg, p->stream,
                          p->timing ? p->ev_stage : nullptr),
           "kernel launch");
     check(cudaEventRecord(p->ev_stop, p->stream), "event");
-    check(cudaMemcpyAsync(p->h_c, p->d_c, bytes, cudaMemcpyDeviceToHost, p->stream), "c copy");
+    const int parts = p->pool->parts();
+    for (int part = 0; part < parts; ++part) {
+        size_t lo, hi;
+        slice(bytes, part, parts, &lo, &hi);
+        if (hi > lo)
+            check(cudaMemcpyAsync(reinterpret_cast<char*>(p->h_c) + lo, reinterpret_cast<char*>(p->d_c) + lo, hi - lo,
+                                  cudaMemcpyDeviceToHost, p->stream),
+                  "product copy");
+        check(cudaEventRecord(p->ev_out[size_t(part)], p->stream), "event");
+    }
+}
+
+void plan_collect_host(Plan* p, uint32_t* c) {
+    if (!p) throw Error(kEInval, "null plan");
+    if (!c) throw Error(kEInval, "null host buffer");
+    const size_t bytes = p->limbs() * sizeof(uint32_t);
+    std::atomic<int> err{int(cudaSuccess)};
+    p->pool->run([&](int part, int parts) {
+        const cudaError_t e = cudaEventSynchronize(p->ev_out[size_t(part)]);
+        if (e != cudaSuccess) {
+            err.store(int(e));
+            return;
+        }
+        size_t lo, hi;
+        slice(bytes, part, parts, &lo, &hi);
+        if (hi > lo)
+            std::memcpy(reinterpret_cast<char*>(c) + lo, reinterpret_cast<const char*>(p->h_c) + lo, hi - lo);
+    });
+    check(cudaError_t(err.load()), "product");
     check(cudaStreamSynchronize(p->stream), "product");
     cudaEventElapsedTime(&p->last_kernel_ms, p->ev_start, p->ev_stop);
-    p->copier->copy(c, p->h_c, bytes);
+}
+
+void plan_multiply_host(Plan* p, const uint32_t* a, const uint32_t* b, uint32_t* c) {
+    plan_submit_host(p, a, b);
+    plan_collect_host(p, c);
+}
+
+// ------------------------------------------------------------------------------ row configuration
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, RowConfig> g_tuned;
+}  // namespace
+
+bool tuned_row_config(int logN, int L, RowConfig* out) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find({logN, L});
+    if (it == g_tuned.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+void plan_set_row_config(Plan* p, const RowConfig& c) {
+    if (!p) throw Error(kEInval, "null plan");
+    if (!row_config_valid(p->logN, c) || !row_variant_exists(c))
+        throw Error(kEInval, "no compiled row kernel for this configuration and N");
+    p->cfg = c;
+}
+
+float plan_autotune(Plan* p, int reps) {
+    if (!p) throw Error(kEInval, "null plan");
+    if (reps < 1) reps = 1;
+    // Operands: the plan's own staging buffers with reduced random limbs (values need not be < q
+    // for timing; every limb pattern runs the same instructions).
+    const size_t words = p->limbs();
+    std::vector<uint32_t> host(words);
+    uint64_t s = 0x9E3779B97F4A7C15ull;
+    for (size_t w = 0; w < words; ++w) {
+        s ^= s << 13;
+        s ^= s >> 7;
+        s ^= s << 17;
+        host[w] = uint32_t(s);
+    }
+    for (size_t n = 0; n < size_t(p->N); ++n) host[n * p->L + p->L - 1] &= p->hq.q[p->L - 1] >> 1;
+    check(cudaMemcpy(p->d_a, host.data(), words * 4, cudaMemcpyHostToDevice), "tune upload");
+    check(cudaMemcpy(p->d_b, host.data(), words * 4, cudaMemcpyHostToDevice), "tune upload");
+    const RowConfig saved = p->cfg;
+    RowConfig best = saved;
+    float best_ms = 1e30f;
+    for (const RowConfig& c : row_variants(p->logN)) {
+        p->cfg = c;
+        const ProductDesc d = p->desc(p->d_a, p->d_b, p->d_c);
+        check(launch_product(d, p->tables->view(), c, p->stream), "tune launch");  // warm-up
+        check(cudaEventRecord(p->ev_start, p->stream), "event");
+        for (int r = 0; r < reps; ++r) check(launch_product(d, p->tables->view(), c, p->stream), "tune launch");
+        check(cudaEventRecord(p->ev_stop, p->stream), "event");
+        check(cudaEventSynchronize(p->ev_stop), "tune");
+        float ms = 0.f;
+        check(cudaEventElapsedTime(&ms, p->ev_start, p->ev_stop), "event");
+        ms /= float(reps);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    p->cfg = best;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[{p->logN, p->L}] = best;
+    return best_ms;
 }
 
 }  // namespace nc

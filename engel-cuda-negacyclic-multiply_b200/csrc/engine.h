@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <condition_variable>
 #include <cstdint>
 #include <functional>
@@ -34,33 +35,32 @@ struct DeviceTables {
     int refs = 0;
     ulonglong2* fwd = nullptr;
     ulonglong2* inv = nullptr;
-    uint64_t* pow32 = nullptr;
-    PrimeConst* pc = nullptr;
-    Tables view() const { return Tables{fwd, inv, pow32, pc}; }
+    Tables view() const { return Tables{fwd, inv}; }
 };
 
 DeviceTables* acquire_tables(int device);
 void release_tables(DeviceTables* t);
 
-// Splits large host memcpys over a few worker threads.
-class ParallelCopy {
+// A few host worker threads that run one job at a time, every thread (workers and the caller)
+// on its own part. Workers spin briefly between jobs, so the back-to-back jobs of one product
+// hand over in microseconds, then sleep.
+class HostPool {
   public:
-    explicit ParallelCopy(int threads);
-    ~ParallelCopy();
-    void copy(void* dst, const void* src, size_t bytes);
-    int threads() const { return int(workers_.size()) + 1; }
+    explicit HostPool(int threads);
+    ~HostPool();
+    int parts() const { return int(workers_.size()) + 1; }
+    // fn(part, parts) on every thread; returns when all parts are done.
+    void run(const std::function<void(int, int)>& fn);
 
   private:
-    void run_part(int part);
+    void worker(int part);
     std::vector<std::thread> workers_;
     std::mutex mu_;
-    std::condition_variable cv_, done_cv_;
-    uint64_t gen_ = 0;
-    int pending_ = 0;
-    bool stop_ = false;
-    char* dst_ = nullptr;
-    const char* src_ = nullptr;
-    size_t bytes_ = 0;
+    std::condition_variable cv_;
+    std::atomic<uint64_t> gen_{0};
+    std::atomic<int> pending_{0};
+    std::atomic<bool> stop_{false};
+    const std::function<void(int, int)>* job_ = nullptr;
 };
 
 // One (N, q) configuration: constants, scratch residues and staging buffers.
@@ -79,9 +79,11 @@ struct Plan {
     uint32_t* h_c = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    std::vector<cudaEvent_t> ev_out;  // one per output chunk (one chunk per pool part)
     DeviceTables* tables = nullptr;
-    ParallelCopy* copier = nullptr;
+    HostPool* pool = nullptr;
     float last_kernel_ms = 0.f;
+    RowConfig cfg{};                 // row-stage tiling of the plain path (autotuned per N)
     bool timing = false;             // record per-stage events
     cudaEvent_t ev_stage[4] = {nullptr, nullptr, nullptr, nullptr};
 
@@ -96,9 +98,25 @@ void plan_destroy(Plan* p);
 // Device-resident product on `stream` (plan stream when null). Asynchronous.
 void plan_multiply_device(Plan* p, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t stream);
 
-// Host buffers in and out (the fherma_run contract). Synchronous.
+// Host buffers in and out (the fherma_run contract), in two halves so a caller can do host work
+// while the GPU computes. submit: every pool thread stages a slice of a and b into pinned memory
+// and enqueues that slice's H2D copy (memcpy and DMA overlap), then the kernels and the chunked
+// D2H are enqueued. collect: each pool thread waits for its output chunk and copies it out.
+void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b);
+void plan_collect_host(Plan* p, uint32_t* c);
 void plan_multiply_host(Plan* p, const uint32_t* a, const uint32_t* b, uint32_t* c);
 
 int current_device();
+
+// Row configuration for the plain path of a plan: validated and applied.
+void plan_set_row_config(Plan* p, const RowConfig& c);
+
+// Times every compiled row configuration valid for the plan's N on its own buffers (`reps`
+// products each, device-resident), applies the fastest and remembers it for later plans of
+// the same (N, L). Returns the best device milliseconds per product.
+float plan_autotune(Plan* p, int reps);
+
+// The remembered choice for (logN, L), if any autotune ran in this process.
+bool tuned_row_config(int logN, int L, RowConfig* out);
 
 }  // namespace nc

@@ -1,0 +1,121 @@
+// Persistent batched kernel: every product of a batch, in one launch.
+//
+// The host lays out a work queue of items (stage, product, index): all residue items of every
+// product, then all row items, then all CRT items. CTAs (as many as fit on the GPU at once)
+// take items in queue order with one atomic. A row item of product p may start once every
+// residue item of p is done, a CRT item once every row item of p is done; the CTA's first
+// thread polls p's counter. Every item a CTA waits for was taken earlier by a CTA that is
+// running and waits on nothing later in the queue, so the waits always end. A wait is still
+// bounded: past kSpinLimit polls (about two seconds) the CTA records an error, skips the
+// item, and every later wait returns at once; the host reports the error after the launch.
+#include "kernel_registry.h"
+#include "stages.cuh"
+
+namespace nc {
+
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Thread 0 only. True once *ctr >= need; false after kSpinLimit polls or once an error is set.
+__device__ bool wait_count(const uint32_t* ctr, uint32_t need, uint32_t* error) {
+    for (uint32_t it = 0; it < kSpinLimit; ++it) {
+        if (ld_acquire(ctr) >= need) return true;
+        if (ld_acquire(error) != 0) return false;
+        __nanosleep(it < 64 ? 64 : 512);
+    }
+    atomicExch(error, 1u);
+    return false;
+}
+
+template <int LW>
+__device__ __forceinline__ void batch_dec(const BatchProduct& bp, const Tables& t, int idx, uint8_t* smem) {
+    const int operand = int(bp.first_operand) + idx / int(bp.tiles);
+    dec_tile<LW>(bp.d, t, operand, idx % int(bp.tiles), smem);
+}
+
+__device__ __forceinline__ void batch_item(uint32_t stage, const BatchProduct& bp, const Tables& t, int idx,
+                                           uint8_t* smem) {
+    if (stage == kItemDec) {
+        switch (bp.d.LW) {
+#define NC_B_DEC(n) \
+    case n: batch_dec<n>(bp, t, idx, smem); break;
+            NC_LW_CASES(NC_B_DEC)
+#undef NC_B_DEC
+            default: break;
+        }
+    } else if (stage == kItemRow) {
+        switch (bp.d.logN2) {
+#define NC_B_ROW(n) \
+    case n: row_blocks<n, 4, kThreads>(bp.d, t, idx, smem); break;
+            NC_B_ROW(1) NC_B_ROW(2) NC_B_ROW(3) NC_B_ROW(4) NC_B_ROW(5) NC_B_ROW(6)
+            NC_B_ROW(7) NC_B_ROW(8) NC_B_ROW(9) NC_B_ROW(10) NC_B_ROW(11) NC_B_ROW(12)
+#undef NC_B_ROW
+            default: break;
+        }
+    } else {
+        switch (bp.d.LW) {
+#define NC_B_CRT(n) \
+    case n: crt_coeffs<n>(bp.d, t, idx, smem); break;
+            NC_LW_CASES(NC_B_CRT)
+#undef NC_B_CRT
+            default: break;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ int s_item;
+    __shared__ int s_go;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = int(atomicAdd(a.head, 1u));
+        __syncthreads();
+        const int it = s_item;
+        if (it >= a.n_items) break;
+        const uint2 w = __ldg(a.items + it);
+        const uint32_t stage = w.x >> 28;
+        const uint32_t prod = w.x & 0x0fffffffu;
+        const BatchProduct bp = a.products[prod];
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            if (stage == kItemRow) ok = wait_count(a.counters + 2 * prod, bp.n_dec, a.error);
+            if (stage == kItemCrt) ok = wait_count(a.counters + 2 * prod + 1, bp.n_row, a.error);
+            s_go = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (s_go) {
+            batch_item(stage, bp, a.tables, int(w.y), smem);
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0 && stage != kItemCrt) atomicAdd(a.counters + 2 * prod + stage, 1u);
+        }
+        __syncthreads();  // s_item / s_go are rewritten by the next round
+    }
+}
+
+cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
+    cudaError_t e = upload_prime_constants(pc, pow32);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(smax(smax(dec_smem_bytes(kMaxPrimes), crt_smem_bytes(kMaxPrimes)),
+                                         row_smem_bytes(kThreads, 4))));
+}
+
+// Launch with `ctas` persistent CTAs and `smem` dynamic shared memory.
+cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s) {
+    BatchArgs a = args;
+    void* params[] = {&a};
+    return cudaLaunchKernel(reinterpret_cast<void*>(&k_persistent), dim3(unsigned(ctas)), dim3(kThreads), params,
+                            smem, s);
+}
+
+cudaError_t persistent_occupancy(size_t smem, int* ctas_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_persistent, kThreads, smem);
+}
+
+}  // namespace nc

@@ -1,0 +1,33 @@
+// Stage 1 kernels: k_dec<LW> (residues + forward column stages), grid = operands x tiles.
+#include "kernel_registry.h"
+#include "stages.cuh"
+
+namespace nc {
+
+template <int LW>
+__global__ void __launch_bounds__(kThreads, 2) k_dec(ProductDesc d, Tables t, int first_operand, int tiles) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int operand = first_operand + int(blockIdx.x) / tiles;
+    const int tile = int(blockIdx.x) % tiles;
+    dec_tile<LW>(d, t, operand, tile, smem);
+}
+
+void* dec_kernel(int LW) {
+    switch (LW) {
+#define NC_DEC(n) \
+    case n: return reinterpret_cast<void*>(&k_dec<n>);
+        NC_LW_CASES(NC_DEC)
+#undef NC_DEC
+        default: return nullptr;
+    }
+}
+
+cudaError_t prepare_dec(const PrimeConst* pc, const uint64_t* pow32) {
+    cudaError_t e = upload_prime_constants(pc, pow32);
+    for (int lw = 2; lw <= kMaxL && e == cudaSuccess; lw += 2)
+        e = cudaFuncSetAttribute(dec_kernel(lw), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(dec_smem_bytes(kMaxPrimes)));
+    return e;
+}
+
+}  // namespace nc

@@ -1,0 +1,27 @@
+// Kernel entry points of the separately compiled kernel translation units. Each unit keeps its
+// own copy of the __constant__ prime tables and uploads it in its prepare function.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "batch_types.h"
+#include "common.h"
+
+namespace nc {
+
+void* dec_kernel(int LW);
+void* crt_kernel(int LW);
+void* row_kernel(const RowConfig& c);
+std::vector<RowConfig> all_row_variants();
+
+cudaError_t prepare_dec(const PrimeConst* pc, const uint64_t* pow32);
+cudaError_t prepare_crt(const PrimeConst* pc, const uint64_t* pow32);
+cudaError_t prepare_row(const PrimeConst* pc, const uint64_t* pow32);
+cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32);
+
+cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s);
+cudaError_t persistent_occupancy(size_t smem, int* ctas_per_sm);
+
+}  // namespace nc

@@ -1,17 +1,20 @@
 // The three stages of one negacyclic product, written as CTA-level device functions so the
 // plain per-call kernels and the persistent batched kernel share them.
 //
-//   stage 1  dec_tile   limbs -> residues mod each prime (solve.cu:533-570 computes the same
+//   stage 1  residues   limbs -> residues mod each prime (solve.cu:533-570 computes the same
 //                       residues) and the first log2(N1) forward NTT stages over columns
-//   stage 2  row_blocks per (prime, row block of N2 residues): forward NTT of a and of b,
+//   stage 2  row blocks per (prime, row block of N2 residues): forward NTT of a and of b,
 //                       pointwise product, inverse NTT (solve.cu:952-1044, 620-628)
-//   stage 3  crt_tile   last log2(N1) inverse stages over columns, then CRT and Barrett
+//   stage 3  CRT        last log2(N1) inverse stages over columns, then CRT and Barrett
 //                       reduction mod q into L limbs (solve.cu:630-642, 752-836)
 //
 // The NTT is the merged negacyclic form: forward Cooley-Tukey with twiddles psi^bitrev(j)
 // (natural order in, bit-reversed order out) and inverse Gentleman-Sande with psi^-bitrev(j)
 // (bit-reversed in, natural out), so no twist, untwist or bit-reversal pass exists. N^-1 is
 // folded into the CRT constant y_i. Residue rows are k x N u64, prime-major.
+//
+// This header defines static __constant__ data: every translation unit that includes it has its
+// own copy and uploads it with upload_prime_constants() before its first launch.
 #pragma once
 
 #include <cstdint>
@@ -21,42 +24,99 @@
 
 namespace nc {
 
-// Device-wide tables (built once per device). Twiddle entry j of prime i sits at
-// fwd[i * kMaxN + j] = (psi^bitrev17(j) ... restricted to the first N), with its Shoup companion.
-struct Tables {
-    const ulonglong2* fwd;    // [kMaxPrimes][kMaxN]
-    const ulonglong2* inv;    // [kMaxPrimes][kMaxN]
-    const uint64_t* pow32;    // [kMaxPrimes][kMaxL]  2^(32 l) mod p_i
-    const PrimeConst* pc;     // [kMaxPrimes]
-};
+// Per-prime constants, read with warp-uniform indices.
+static __constant__ PrimeConst c_pc[kMaxPrimes];
+static __constant__ uint64_t c_pow32[kMaxPrimes * kMaxL];  // 2^(32 l) mod p_i
 
-// ------------------------------------------------------------------------------------------
-// shared-memory sizes
+static inline cudaError_t upload_prime_constants(const PrimeConst* pc, const uint64_t* pow32) {
+    cudaError_t e = cudaMemcpyToSymbol(c_pc, pc, sizeof(PrimeConst) * kMaxPrimes);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_pow32, pow32, sizeof(uint64_t) * kMaxPrimes * kMaxL);
+    return e;
+}
 
-__host__ __device__ constexpr size_t dec_smem_bytes() {
-    return size_t(kTile) * kMaxL * 4 + size_t(kMaxPrimes) * kMaxL * 8;
-}
-__host__ __device__ constexpr size_t row_smem_bytes() { return size_t(2) << kRowLogMax << 3; }
-__host__ __device__ constexpr size_t crt_smem_bytes(int k) {
-    return size_t(kTile) * 8 * (k > 16 ? k : 16)        // residues (>= output staging 256*32*4)
-           + size_t(k) * kMqStride * 4                 // M/p_i mod q
-           + size_t(k) * 8 * 3                         // y, y shoup, p
-           + size_t(k) * 4                             // g
-           + size_t(kMqStride) * 4 * 2 + 16;           // -M mod q, q, mu
-}
-__host__ __device__ constexpr size_t max_smem_bytes() {
-    return crt_smem_bytes(kMaxPrimes) > row_smem_bytes()
-               ? (crt_smem_bytes(kMaxPrimes) > dec_smem_bytes() ? crt_smem_bytes(kMaxPrimes) : dec_smem_bytes())
-               : (row_smem_bytes() > dec_smem_bytes() ? row_smem_bytes() : dec_smem_bytes());
-}
+#define NC_LW_CASES(X) X(2) X(4) X(6) X(8) X(10) X(12) X(14) X(16) X(18) X(20) X(22) X(24) X(26) X(28) X(30) X(32)
 
 // ------------------------------------------------------------------------------------------
 // stage 1: residues + forward column stages
 
+// Loads the CTA's tile (N1 segments of C consecutive coefficients) into shared memory.
+__device__ __forceinline__ void load_tile(const uint32_t* x, int N2, int L, int j0, int C, int N1,
+                                          uint32_t* s_in) {
+    const int seg = C * L;
+    for (int u = 0; u < N1; ++u) {
+        const size_t first = (size_t(u) * N2 + j0) * L;
+        const uint32_t* src = x + first;
+        uint32_t* dst = s_in + u * seg;
+        if (((first | size_t(seg)) & 3) == 0) {
+            const uint4* s4 = reinterpret_cast<const uint4*>(src);
+            uint4* d4 = reinterpret_cast<uint4*>(dst);
+            for (int w = threadIdx.x; w < (seg >> 2); w += blockDim.x) d4[w] = __ldg(s4 + w);
+        } else {
+            for (int w = threadIdx.x; w < seg; w += blockDim.x) dst[w] = __ldg(src + w);
+        }
+    }
+}
+
+// Thread t owns coefficient t of the tile: its limbs stay in registers while it walks the
+// primes two at a time (two independent carry chains), writing residues in [0, 2p) to
+// s_res[i * T + t]. s_res overlays the limb tile, so the limbs are read first.
+template <int LW>
+__device__ __forceinline__ void dec_residues(const uint32_t* s_in, int L, int k, int T, uint64_t* s_res) {
+    const int t = threadIdx.x;
+    const bool active = t < T;
+    uint32_t x[LW];
+#pragma unroll
+    for (int l = 0; l < LW; ++l) x[l] = 0;
+    if (active) {
+        const uint32_t* src = s_in + t * L;
+        if ((L & 3) == 0) {
+#pragma unroll
+            for (int l = 0; l < LW; l += 4)
+                if (l < L) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(src + l);
+                    x[l] = v.x;
+                    x[l + 1] = v.y;
+                    x[l + 2] = v.z;
+                    x[l + 3] = v.w;
+                }
+        } else if ((L & 1) == 0) {
+#pragma unroll
+            for (int l = 0; l < LW; l += 2)
+                if (l < L) {
+                    const uint2 v = *reinterpret_cast<const uint2*>(src + l);
+                    x[l] = v.x;
+                    x[l + 1] = v.y;
+                }
+        } else {
+#pragma unroll
+            for (int l = 0; l < LW; ++l)
+                if (l < L) x[l] = src[l];
+        }
+    }
+    __syncthreads();  // the limb tile is in registers; s_res may now overwrite it
+    if (!active) return;
+#pragma unroll 1
+    for (int i = 0; i < k; i += 2) {
+        const int i2 = (i + 1 < k) ? i + 1 : i;
+        const uint64_t* c1 = c_pow32 + i * kMaxL;
+        const uint64_t* c2 = c_pow32 + i2 * kMaxL;
+        uint32_t a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
+        uint32_t e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;
+#pragma unroll
+        for (int l = 0; l < LW; ++l) {
+            const uint64_t c = c1[l], dd = c2[l];
+            mac_u32x64(x[l], uint32_t(c), uint32_t(c >> 32), a0, a1, a2, b0, b1, b2);
+            mac_u32x64(x[l], uint32_t(dd), uint32_t(dd >> 32), e0, e1, e2, f0, f1, f2);
+        }
+        s_res[size_t(i) * T + t] = reduce_limb_sum(a0, a1, a2, b0, b1, b2, c_pc[i].m);
+        if (i + 1 < k) s_res[size_t(i2) * T + t] = reduce_limb_sum(e0, e1, e2, f0, f1, f2, c_pc[i2].m);
+    }
+}
+
+// Forward column stages (global stages m = 1 .. N1/2) of one column held in registers.
 template <int LOG_N1>
-__device__ __forceinline__ void dec_column(const Tables& t, int i, uint64_t p, uint64_t (&v)[1 << LOG_N1]) {
+__device__ __forceinline__ void column_forward(const ulonglong2* tw, uint64_t p, uint64_t (&v)[1 << LOG_N1]) {
     constexpr int N1 = 1 << LOG_N1;
-    const ulonglong2* tw = t.fwd + size_t(i) * kMaxN;
     const uint64_t p2 = 2 * p;
 #pragma unroll
     for (int s = 0; s < LOG_N1; ++s) {
@@ -73,97 +133,69 @@ __device__ __forceinline__ void dec_column(const Tables& t, int i, uint64_t p, u
     }
 }
 
-// Sum_l limb_l * 2^(32 l) mod p for one coefficient held in shared memory; result in [0, 2p).
-template <int VEC>
-__device__ __forceinline__ uint64_t residue_of(const uint32_t* limbs, const uint64_t* pw, int L, uint64_t m) {
-    uint32_t a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
-    if (VEC == 4) {
-#pragma unroll 1
-        for (int l = 0; l < L; l += 4) {
-            const uint4 x = *reinterpret_cast<const uint4*>(limbs + l);
-            const uint64_t c0 = pw[l], c1 = pw[l + 1], c2 = pw[l + 2], c3 = pw[l + 3];
-            mac_u32x64(x.x, uint32_t(c0), uint32_t(c0 >> 32), a0, a1, a2, b0, b1, b2);
-            mac_u32x64(x.y, uint32_t(c1), uint32_t(c1 >> 32), a0, a1, a2, b0, b1, b2);
-            mac_u32x64(x.z, uint32_t(c2), uint32_t(c2 >> 32), a0, a1, a2, b0, b1, b2);
-            mac_u32x64(x.w, uint32_t(c3), uint32_t(c3 >> 32), a0, a1, a2, b0, b1, b2);
-        }
-    } else if (VEC == 2) {
-#pragma unroll 1
-        for (int l = 0; l < L; l += 2) {
-            const uint2 x = *reinterpret_cast<const uint2*>(limbs + l);
-            const uint64_t c0 = pw[l], c1 = pw[l + 1];
-            mac_u32x64(x.x, uint32_t(c0), uint32_t(c0 >> 32), a0, a1, a2, b0, b1, b2);
-            mac_u32x64(x.y, uint32_t(c1), uint32_t(c1 >> 32), a0, a1, a2, b0, b1, b2);
-        }
-    } else {
-#pragma unroll 1
-        for (int l = 0; l < L; ++l) {
-            const uint64_t c0 = pw[l];
-            mac_u32x64(limbs[l], uint32_t(c0), uint32_t(c0 >> 32), a0, a1, a2, b0, b1, b2);
+// Inverse column stages (global stages m = N1/2 .. 1) of one column held in registers.
+template <int LOG_N1>
+__device__ __forceinline__ void column_inverse(const ulonglong2* tw, uint64_t p, uint64_t (&v)[1 << LOG_N1]) {
+    constexpr int N1 = 1 << LOG_N1;
+    const uint64_t p2 = 2 * p;
+#pragma unroll
+    for (int s = LOG_N1 - 1; s >= 0; --s) {
+        const int half = N1 >> (s + 1);
+#pragma unroll
+        for (int blk = 0; blk < (1 << s); ++blk) {
+            const ulonglong2 w = __ldg(tw + (1 << s) + blk);
+#pragma unroll
+            for (int jj = 0; jj < half; ++jj) {
+                const int u = blk * 2 * half + jj;
+                gs_bfly(v[u], v[u + half], w.x, w.y, p, p2);
+            }
         }
     }
-    // S = (a2:a1:a0) + (b2:b1:b0) * 2^32 < 2^99
-    const uint64_t lo_a = (uint64_t(a1) << 32) | a0;
-    const uint64_t mid = uint64_t(b1) << 32 | b0;  // contributes mid * 2^32
-    const uint64_t add_lo = mid << 32;
-    const uint64_t lo = lo_a + add_lo;
-    const uint64_t hi = uint64_t(a2) + (mid >> 32) + (uint64_t(b2) << 32) + (lo < lo_a ? 1u : 0u);
-    return reduce_special(hi, lo, m);
 }
 
+// Items (prime i, column j) of the tile: column transform from s_res, store the residue rows.
 template <int LOG_N1>
-__device__ void dec_tile(const ProductDesc& d, const Tables& t, int operand, int tile, uint8_t* smem) {
+__device__ void dec_columns(const Tables& t, int k, int N, int T, int j0, const uint64_t* s_res, uint64_t* R) {
     constexpr int N1 = 1 << LOG_N1;
-    const int N = 1 << d.logN;
-    const int N2 = N >> LOG_N1;
-    const int T = N < kTile ? N : kTile;
     const int C = T >> LOG_N1;
+    const int N2 = N >> LOG_N1;
+    for (int w = threadIdx.x; w < k * C; w += blockDim.x) {
+        const int i = w / C, j = w - i * C;
+        uint64_t v[N1];
+#pragma unroll
+        for (int u = 0; u < N1; ++u) v[u] = s_res[size_t(i) * T + u * C + j];
+        if (LOG_N1 > 0) column_forward<LOG_N1>(t.fwd + size_t(i) * kMaxN, c_pc[i].p, v);
+        uint64_t* row = R + size_t(i) * N + j0 + j;
+#pragma unroll
+        for (int u = 0; u < N1; ++u) __stcg(row + size_t(u) * N2, v[u]);
+    }
+}
+
+template <int LW>
+__device__ void dec_tile(const ProductDesc& d, const Tables& t, int operand, int tile, uint8_t* smem) {
+    const int N = 1 << d.logN;
+    const int logN1 = int(d.logN) - int(d.logN2);
+    const int T = N < kTile ? N : kTile;
+    const int C = T >> logN1;
     const int L = int(d.L), k = int(d.k);
     const uint32_t* x = operand ? d.b : d.a;
     uint64_t* R = operand ? d.rb : d.ra;
     uint32_t* s_in = reinterpret_cast<uint32_t*>(smem);
-    uint64_t* s_pow = reinterpret_cast<uint64_t*>(smem + size_t(kTile) * kMaxL * 4);
+    uint64_t* s_res = reinterpret_cast<uint64_t*>(smem);
     const int j0 = tile * C;
-    const int seg = C * L;
 
     __syncthreads();  // the previous user of shared memory (persistent CTAs) is done
-    for (int u = 0; u < N1; ++u) {
-        const size_t first = (size_t(u) * N2 + j0) * L;
-        const uint32_t* src = x + first;
-        uint32_t* dst = s_in + u * seg;
-        if (((first | size_t(seg)) & 3) == 0) {
-            const uint4* s4 = reinterpret_cast<const uint4*>(src);
-            uint4* d4 = reinterpret_cast<uint4*>(dst);
-            for (int w = threadIdx.x; w < (seg >> 2); w += kThreads) d4[w] = __ldg(s4 + w);
-        } else {
-            for (int w = threadIdx.x; w < seg; w += kThreads) dst[w] = __ldg(src + w);
-        }
-    }
-    for (int w = threadIdx.x; w < k * L; w += kThreads) {
-        const int i = w / L, l = w - i * L;
-        s_pow[w] = __ldg(t.pow32 + i * kMaxL + l);
-    }
+    load_tile(x, N >> logN1, L, j0, C, 1 << logN1, s_in);
     __syncthreads();
-
-    for (int w = threadIdx.x; w < k * C; w += kThreads) {
-        const int i = w / C, j = w - i * C;
-        const uint64_t p = __ldg(&t.pc[i].p), m = __ldg(&t.pc[i].m);
-        const uint64_t* pw = s_pow + i * L;
-        uint64_t v[N1];
-#pragma unroll
-        for (int u = 0; u < N1; ++u) {
-            const uint32_t* limbs = s_in + u * seg + j * L;
-            if ((L & 3) == 0)
-                v[u] = residue_of<4>(limbs, pw, L, m);
-            else if ((L & 1) == 0)
-                v[u] = residue_of<2>(limbs, pw, L, m);
-            else
-                v[u] = residue_of<1>(limbs, pw, L, m);
-        }
-        dec_column<LOG_N1>(t, i, p, v);
-        uint64_t* row = R + size_t(i) * N + j0 + j;
-#pragma unroll
-        for (int u = 0; u < N1; ++u) row[size_t(u) * N2] = v[u];
+    dec_residues<LW>(s_in, L, k, T, s_res);
+    __syncthreads();
+    switch (logN1) {
+        case 0: dec_columns<0>(t, k, N, T, j0, s_res, R); break;
+        case 1: dec_columns<1>(t, k, N, T, j0, s_res, R); break;
+        case 2: dec_columns<2>(t, k, N, T, j0, s_res, R); break;
+        case 3: dec_columns<3>(t, k, N, T, j0, s_res, R); break;
+        case 4: dec_columns<4>(t, k, N, T, j0, s_res, R); break;
+        default: dec_columns<5>(t, k, N, T, j0, s_res, R); break;
     }
 }
 
@@ -177,36 +209,34 @@ __device__ __forceinline__ int swz(int x) {
     return (pc << 1) | (x & 1);
 }
 
-template <int LOG_N2>
+template <int LOG_N2_, int LOG_E>
 struct RowShape {
+    static constexpr int LOG_N2 = LOG_N2_;
     static constexpr int N2 = 1 << LOG_N2;
-    static constexpr int LOG_E = LOG_N2 < 4 ? LOG_N2 : 4;
-    static constexpr int E = 1 << LOG_E;
-    static constexpr int T = N2 / E;                     // threads per row block
-    static constexpr int ROWS = kThreads / T;            // row blocks per CTA
-    static constexpr int NPASS = (LOG_N2 + LOG_E - 1) / LOG_E;
-    __host__ __device__ static constexpr int l0(int pass) { return pass * LOG_E; }
+    static constexpr int LE = LOG_N2 < LOG_E ? LOG_N2 : LOG_E;
+    static constexpr int E = 1 << LE;
+    static constexpr int T = N2 / E;  // threads per row block
+    static constexpr int NPASS = (LOG_N2 + LE - 1) / LE;
+    __host__ __device__ static constexpr int l0(int pass) { return pass * LE; }
     __host__ __device__ static constexpr int r(int pass) {
-        return (LOG_N2 - pass * LOG_E) < LOG_E ? (LOG_N2 - pass * LOG_E) : LOG_E;
+        return (LOG_N2 - pass * LE) < LE ? (LOG_N2 - pass * LE) : LE;
     }
     __host__ __device__ static constexpr int lolog(int pass) { return LOG_N2 - l0(pass) - r(pass); }
 };
 
-// Element index (inside the row block) of register slot e in pass `pass` for thread lt.
-template <int LOG_N2, int PASS>
+// Element index (inside the row block) of register slot e in pass PASS for thread lt.
+// A pass runs r stages on groups of 2^r elements x = hi * (N2 >> l0) + s * 2^lolog + lo.
+template <class S, int PASS>
 __device__ __forceinline__ int row_index(int lt, int e) {
-    using S = RowShape<LOG_N2>;
     constexpr int R = S::r(PASS), LL = S::lolog(PASS);
     const int q = e >> R, s = e & ((1 << R) - 1);
     const int g = lt + S::T * q;
     const int hi = g >> LL, lo = g & ((1 << LL) - 1);
-    return (hi << (LOG_N2 - S::l0(PASS))) + (s << LL) + lo;
+    return (hi << (S::LOG_N2 - S::l0(PASS))) + (s << LL) + lo;
 }
 
-template <int LOG_N2, int PASS, bool FWD>
-__device__ __forceinline__ void row_pass(uint64_t (&v)[RowShape<LOG_N2>::E], const ulonglong2* tw, int base, int lt,
-                                         uint64_t p) {
-    using S = RowShape<LOG_N2>;
+template <class S, int PASS, bool FWD>
+__device__ __forceinline__ void row_pass(uint64_t (&v)[S::E], const ulonglong2* tw, int base, int lt, uint64_t p) {
     constexpr int R = S::r(PASS), LL = S::lolog(PASS), L0 = S::l0(PASS);
     const uint64_t p2 = 2 * p;
 #pragma unroll
@@ -217,14 +247,14 @@ __device__ __forceinline__ void row_pass(uint64_t (&v)[RowShape<LOG_N2>::E], con
         for (int jj = 0; jj < R; ++jj) {
             const int j = FWD ? jj : R - 1 - jj;
             const int half = 1 << (R - 1 - j);
+            // twiddle of local stage l = L0 + j, block b: (N1 + u) 2^l + hi 2^j + (s >> (R - j))
             const int twbase = (base << (L0 + j)) + (hi << j);
 #pragma unroll
             for (int blk = 0; blk < (1 << j); ++blk) {
                 const ulonglong2 w = __ldg(tw + twbase + blk);
 #pragma unroll
                 for (int s0 = 0; s0 < half; ++s0) {
-                    const int s = blk * 2 * half + s0;
-                    const int e = q * (1 << R) + s;
+                    const int e = q * (1 << R) + blk * 2 * half + s0;
                     if (FWD)
                         ct_bfly(v[e], v[e + half], w.x, w.y, p, p2);
                     else
@@ -235,85 +265,84 @@ __device__ __forceinline__ void row_pass(uint64_t (&v)[RowShape<LOG_N2>::E], con
     }
 }
 
-template <int LOG_N2, int PASS>
-__device__ __forceinline__ void row_store(const uint64_t (&v)[RowShape<LOG_N2>::E], uint64_t* buf, int lt) {
-    using S = RowShape<LOG_N2>;
+template <class S, int PASS>
+__device__ __forceinline__ void row_store(const uint64_t (&v)[S::E], uint64_t* buf, int lt) {
     if (S::lolog(PASS) == 0 && S::r(PASS) >= 1) {
 #pragma unroll
         for (int e = 0; e < S::E; e += 2) {
-            const int x = row_index<LOG_N2, PASS>(lt, e);
+            const int x = row_index<S, PASS>(lt, e);
             reinterpret_cast<ulonglong2*>(buf)[swz(x) >> 1] = make_ulonglong2(v[e], v[e + 1]);
         }
     } else {
 #pragma unroll
-        for (int e = 0; e < S::E; ++e) buf[swz(row_index<LOG_N2, PASS>(lt, e))] = v[e];
+        for (int e = 0; e < S::E; ++e) buf[swz(row_index<S, PASS>(lt, e))] = v[e];
     }
 }
 
-template <int LOG_N2, int PASS>
-__device__ __forceinline__ void row_load(uint64_t (&v)[RowShape<LOG_N2>::E], const uint64_t* buf, int lt) {
-    using S = RowShape<LOG_N2>;
+template <class S, int PASS>
+__device__ __forceinline__ void row_load(uint64_t (&v)[S::E], const uint64_t* buf, int lt) {
     if (S::lolog(PASS) == 0 && S::r(PASS) >= 1) {
 #pragma unroll
         for (int e = 0; e < S::E; e += 2) {
-            const int x = row_index<LOG_N2, PASS>(lt, e);
+            const int x = row_index<S, PASS>(lt, e);
             const ulonglong2 pr = reinterpret_cast<const ulonglong2*>(buf)[swz(x) >> 1];
             v[e] = pr.x;
             v[e + 1] = pr.y;
         }
     } else {
 #pragma unroll
-        for (int e = 0; e < S::E; ++e) v[e] = buf[swz(row_index<LOG_N2, PASS>(lt, e))];
+        for (int e = 0; e < S::E; ++e) v[e] = buf[swz(row_index<S, PASS>(lt, e))];
     }
 }
 
-// Forward passes 0..NPASS-1 starting from registers in pass-0 layout; ends in last-pass layout.
-template <int LOG_N2, int PASS>
-__device__ __forceinline__ void row_forward_from(uint64_t (&v)[RowShape<LOG_N2>::E], uint64_t* buf,
-                                                 const ulonglong2* tw, int base, int lt, uint64_t p) {
-    using S = RowShape<LOG_N2>;
-    row_pass<LOG_N2, PASS, true>(v, tw, base, lt, p);
+// Forward passes PASS..NPASS-1 from registers in pass-PASS layout; ends in last-pass layout.
+template <class S, int PASS>
+__device__ __forceinline__ void row_forward_from(uint64_t (&v)[S::E], uint64_t* buf, const ulonglong2* tw,
+                                                 int base, int lt, uint64_t p) {
+    row_pass<S, PASS, true>(v, tw, base, lt, p);
     if constexpr (PASS + 1 < S::NPASS) {
         __syncthreads();
-        row_store<LOG_N2, PASS>(v, buf, lt);
+        row_store<S, PASS>(v, buf, lt);
         __syncthreads();
-        row_load<LOG_N2, PASS + 1>(v, buf, lt);
-        row_forward_from<LOG_N2, PASS + 1>(v, buf, tw, base, lt, p);
+        row_load<S, PASS + 1>(v, buf, lt);
+        row_forward_from<S, PASS + 1>(v, buf, tw, base, lt, p);
     }
 }
 
-// Inverse passes PASS..0 starting from registers in pass-PASS layout; ends in pass-0 layout.
-template <int LOG_N2, int PASS>
-__device__ __forceinline__ void row_inverse_from(uint64_t (&v)[RowShape<LOG_N2>::E], uint64_t* buf,
-                                                 const ulonglong2* tw, int base, int lt, uint64_t p) {
-    row_pass<LOG_N2, PASS, false>(v, tw, base, lt, p);
+// Inverse passes PASS..0 from registers in pass-PASS layout; ends in pass-0 layout.
+template <class S, int PASS>
+__device__ __forceinline__ void row_inverse_from(uint64_t (&v)[S::E], uint64_t* buf, const ulonglong2* tw,
+                                                 int base, int lt, uint64_t p) {
+    row_pass<S, PASS, false>(v, tw, base, lt, p);
     if constexpr (PASS > 0) {
         __syncthreads();
-        row_store<LOG_N2, PASS>(v, buf, lt);
+        row_store<S, PASS>(v, buf, lt);
         __syncthreads();
-        row_load<LOG_N2, PASS - 1>(v, buf, lt);
-        row_inverse_from<LOG_N2, PASS - 1>(v, buf, tw, base, lt, p);
+        row_load<S, PASS - 1>(v, buf, lt);
+        row_inverse_from<S, PASS - 1>(v, buf, tw, base, lt, p);
     }
 }
 
-// One CTA handles ROWS row blocks: block rb = item * ROWS + (tid / T) is prime rb >> logN1,
-// row u = rb & (N1 - 1), residues [u * N2, (u + 1) * N2) of that prime's row.
-template <int LOG_N2>
+// One CTA of THREADS threads handles ROWS = THREADS / T row blocks: block rb = item * ROWS +
+// (tid / T) is prime rb >> logN1, row u = rb & (N1 - 1), residues [u N2, (u + 1) N2).
+template <int LOG_N2, int LOG_E, int THREADS>
 __device__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint8_t* smem) {
-    using S = RowShape<LOG_N2>;
+    using S = RowShape<LOG_N2, LOG_E>;
+    static_assert(S::T <= THREADS, "row block needs more threads than the CTA has");
+    constexpr int ROWS = THREADS / S::T;
     constexpr int LAST = S::NPASS - 1;
     const int logN1 = int(d.logN) - LOG_N2;
     const int N = 1 << d.logN;
     const int rr = threadIdx.x / S::T, lt = threadIdx.x - rr * S::T;
-    const int rb = item * S::ROWS + rr;
+    const int rb = item * ROWS + rr;
     const bool active = rb < (int(d.k) << logN1);
     const int i = active ? rb >> logN1 : 0;
     const int u = rb & ((1 << logN1) - 1);
-    const uint64_t p = __ldg(&t.pc[i].p), m = __ldg(&t.pc[i].m);
-    const int base = (1 << logN1) + u;  // (N1 + u): twiddle index of local stage l is base << l + ...
+    const uint64_t p = c_pc[i].p, m = c_pc[i].m;
+    const int base = (1 << logN1) + u;
     const size_t off = size_t(i) * N + size_t(u) * S::N2;
     uint64_t* buf = reinterpret_cast<uint64_t*>(smem) + rr * S::N2;
-    uint64_t* buf_a = reinterpret_cast<uint64_t*>(smem) + (size_t(S::ROWS) << LOG_N2) + rr * S::N2;
+    uint64_t* buf_a = reinterpret_cast<uint64_t*>(smem) + size_t(ROWS) * S::N2 + rr * S::N2;
     const ulonglong2* twf = t.fwd + size_t(i) * kMaxN;
     const ulonglong2* twi = t.inv + size_t(i) * kMaxN;
     uint64_t v[S::E];
@@ -323,41 +352,52 @@ __device__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint
         // a is already in the NTT domain: stage it into buf_a
 #pragma unroll
         for (int e = 0; e < S::E; ++e) {
-            const int x = row_index<LOG_N2, 0>(lt, e);
+            const int x = row_index<S, 0>(lt, e);
             buf_a[swz(x)] = active ? __ldcg(d.a_hat + off + x) : 0;
         }
     } else {
 #pragma unroll
-        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(d.ra + off + row_index<LOG_N2, 0>(lt, e)) : 0;
-        row_forward_from<LOG_N2, 0>(v, buf, twf, base, lt, p);
+        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(d.ra + off + row_index<S, 0>(lt, e)) : 0;
+        row_forward_from<S, 0>(v, buf, twf, base, lt, p);
         if (d.mode == kModeForward) {
             __syncthreads();
-            row_store<LOG_N2, LAST>(v, buf, lt);
+            row_store<S, LAST>(v, buf, lt);
             __syncthreads();
-            row_load<LOG_N2, 0>(v, buf, lt);
+            row_load<S, 0>(v, buf, lt);
             if (active) {
 #pragma unroll
-                for (int e = 0; e < S::E; ++e) __stcg(d.hat_out + off + row_index<LOG_N2, 0>(lt, e), v[e]);
+                for (int e = 0; e < S::E; ++e) __stcg(d.hat_out + off + row_index<S, 0>(lt, e), v[e]);
             }
             return;
         }
-        row_store<LOG_N2, LAST>(v, buf_a, lt);
+        row_store<S, LAST>(v, buf_a, lt);
     }
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(d.rb + off + row_index<LOG_N2, 0>(lt, e)) : 0;
-    row_forward_from<LOG_N2, 0>(v, buf, twf, base, lt, p);
+    for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(d.rb + off + row_index<S, 0>(lt, e)) : 0;
+    row_forward_from<S, 0>(v, buf, twf, base, lt, p);
     __syncthreads();
     {
-        uint64_t av[S::E];
-        row_load<LOG_N2, LAST>(av, buf_a, lt);
         const uint64_t p2 = 2 * p;
+        if (S::lolog(LAST) == 0 && S::r(LAST) >= 1) {
 #pragma unroll
-        for (int e = 0; e < S::E; ++e) v[e] = mulmod_special(csub(csub(av[e], p2), p), v[e], m);
+            for (int e = 0; e < S::E; e += 2) {
+                const int x = row_index<S, LAST>(lt, e);
+                const ulonglong2 pr = reinterpret_cast<const ulonglong2*>(buf_a)[swz(x) >> 1];
+                v[e] = mulmod_special(csub(csub(pr.x, p2), p), v[e], m);
+                v[e + 1] = mulmod_special(csub(csub(pr.y, p2), p), v[e + 1], m);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < S::E; ++e) {
+                const uint64_t av = buf_a[swz(row_index<S, LAST>(lt, e))];
+                v[e] = mulmod_special(csub(csub(av, p2), p), v[e], m);
+            }
+        }
     }
-    row_inverse_from<LOG_N2, LAST>(v, buf, twi, base, lt, p);
+    row_inverse_from<S, LAST>(v, buf, twi, base, lt, p);
     if (active) {
 #pragma unroll
-        for (int e = 0; e < S::E; ++e) __stcg(d.ra + off + row_index<LOG_N2, 0>(lt, e), v[e]);
+        for (int e = 0; e < S::E; ++e) __stcg(d.ra + off + row_index<S, 0>(lt, e), v[e]);
     }
 }
 
@@ -373,58 +413,45 @@ __device__ void crt_columns(const ProductDesc& d, const Tables& t, int tile, uin
     const int C = T >> LOG_N1;
     const int k = int(d.k);
     const int j0 = tile * C;
-    for (int w = threadIdx.x; w < k * C; w += kThreads) {
+    for (int w = threadIdx.x; w < k * C; w += blockDim.x) {
         const int i = w / C, j = w - i * C;
-        const uint64_t p = __ldg(&t.pc[i].p);
-        const uint64_t p2 = 2 * p;
         const uint64_t* row = d.ra + size_t(i) * N + j0 + j;
         uint64_t v[N1];
 #pragma unroll
         for (int u = 0; u < N1; ++u) v[u] = __ldcg(row + size_t(u) * N2);
-        const ulonglong2* tw = t.inv + size_t(i) * kMaxN;
-#pragma unroll
-        for (int s = LOG_N1 - 1; s >= 0; --s) {
-            const int half = N1 >> (s + 1);
-#pragma unroll
-            for (int blk = 0; blk < (1 << s); ++blk) {
-                const ulonglong2 wv = __ldg(tw + (1 << s) + blk);
-#pragma unroll
-                for (int jj = 0; jj < half; ++jj) {
-                    const int uu = blk * 2 * half + jj;
-                    gs_bfly(v[uu], v[uu + half], wv.x, wv.y, p, p2);
-                }
-            }
-        }
+        if (LOG_N1 > 0) column_inverse<LOG_N1>(t.inv + size_t(i) * kMaxN, c_pc[i].p, v);
 #pragma unroll
         for (int u = 0; u < N1; ++u) s_res[size_t(i) * T + u * C + j] = v[u];
     }
 }
 
-// acc[OFF..W) += v * M[0..LW)  (carry chains; the top word absorbs the final carry)
+// acc[OFF..W) += lo(v * M[l]) placed at word OFF + l  (one carry chain; top word takes the carry)
 template <int LW, int OFF, int W>
-__device__ __forceinline__ void mac_row(uint32_t (&acc)[W], const uint32_t* M, uint32_t v) {
+__device__ __forceinline__ void mac_lo(uint32_t (&acc)[W], const uint32_t* M, uint32_t v) {
     asm volatile("mad.lo.cc.u32 %0, %1, %2, %0;" : "+r"(acc[OFF]) : "r"(v), "r"(M[0]));
 #pragma unroll
     for (int l = 1; l < LW; ++l) asm volatile("madc.lo.cc.u32 %0, %1, %2, %0;" : "+r"(acc[OFF + l]) : "r"(v), "r"(M[l]));
 #pragma unroll
     for (int w = OFF + LW; w < W - 1; ++w) asm volatile("addc.cc.u32 %0, %0, 0;" : "+r"(acc[w]));
     asm volatile("addc.u32 %0, %0, 0;" : "+r"(acc[W - 1]));
-    asm volatile("mad.hi.cc.u32 %0, %1, %2, %0;" : "+r"(acc[OFF + 1]) : "r"(v), "r"(M[0]));
-#pragma unroll
-    for (int l = 1; l < LW; ++l)
-        asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(acc[OFF + 1 + l]) : "r"(v), "r"(M[l]));
-#pragma unroll
-    for (int w = OFF + 1 + LW; w < W - 1; ++w) asm volatile("addc.cc.u32 %0, %0, 0;" : "+r"(acc[w]));
-    if (OFF + 1 + LW < W) asm volatile("addc.u32 %0, %0, 0;" : "+r"(acc[W - 1]));
 }
 
-__device__ __forceinline__ uint32_t funnel(uint32_t lo, uint32_t hi, int sh) {
-    return __funnelshift_r(lo, hi, sh);
+// acc[OFF..W) += hi(v * M[l]) placed at word OFF + l
+template <int LW, int OFF, int W>
+__device__ __forceinline__ void mac_hi(uint32_t (&acc)[W], const uint32_t* M, uint32_t v) {
+    asm volatile("mad.hi.cc.u32 %0, %1, %2, %0;" : "+r"(acc[OFF]) : "r"(v), "r"(M[0]));
+#pragma unroll
+    for (int l = 1; l < LW; ++l) asm volatile("madc.hi.cc.u32 %0, %1, %2, %0;" : "+r"(acc[OFF + l]) : "r"(v), "r"(M[l]));
+#pragma unroll
+    for (int w = OFF + LW; w < W - 1; ++w) asm volatile("addc.cc.u32 %0, %0, 0;" : "+r"(acc[w]));
+    if (OFF + LW < W) asm volatile("addc.u32 %0, %0, 0;" : "+r"(acc[W - 1]));
 }
 
-// r (LW + 1 words) := acc mod q, for acc < 2^(qbits + kBarrettT). q_top = index of q's top word.
+__device__ __forceinline__ uint32_t funnel(uint32_t lo, uint32_t hi, int sh) { return __funnelshift_r(lo, hi, sh); }
+
+// r (LW + 1 words) := acc mod q, for acc < 2^(qbits + kBarrettT).
 template <int LW, int W>
-__device__ __forceinline__ void barrett(uint32_t (&acc)[W], const uint32_t* q, const uint32_t* mu, int qbits,
+__device__ __forceinline__ void barrett(const uint32_t (&acc)[W], const uint32_t* q, const uint32_t* mu, int qbits,
                                         uint32_t (&r)[LW + 1]) {
     // y = floor(acc / 2^(qbits-1)): 3 words. qbits - 1 lies in [32 (L-1), 32 L), L in {LW-1, LW}.
     const int b1 = qbits - 1;
@@ -440,40 +467,36 @@ __device__ __forceinline__ void barrett(uint32_t (&acc)[W], const uint32_t* q, c
         y2 = funnel(acc[LW], acc[LW + 1], sh);
     }
     // t = y * mu (6 words), qh = t >> (kBarrettT + 2) = t >> 71
-    const uint32_t m0 = mu[0], m1 = mu[1], m2 = mu[2];
-    uint32_t t[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t tt[6] = {0, 0, 0, 0, 0, 0};
     {
         const uint32_t ys[3] = {y0, y1, y2};
+        const uint32_t ms[3] = {mu[0], mu[1], mu[2]};
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             uint64_t carry = 0;
-            const uint32_t ms[3] = {m0, m1, m2};
 #pragma unroll
             for (int bb = 0; bb < 3; ++bb) {
-                const uint64_t cur = uint64_t(t[a + bb]) + uint64_t(ys[a]) * ms[bb] + carry;
-                t[a + bb] = uint32_t(cur);
+                const uint64_t cur = uint64_t(tt[a + bb]) + uint64_t(ys[a]) * ms[bb] + carry;
+                tt[a + bb] = uint32_t(cur);
                 carry = cur >> 32;
             }
-            t[a + 3] = uint32_t(carry);
+            tt[a + 3] = uint32_t(carry);
         }
     }
-    const uint32_t q0 = funnel(t[2], t[3], 7), q1 = funnel(t[3], t[4], 7), q2 = funnel(t[4], t[5], 7);
-    // prod = (q2:q1:q0) * q, low LW + 1 words
+    const uint32_t qs[3] = {funnel(tt[2], tt[3], 7), funnel(tt[3], tt[4], 7), funnel(tt[4], tt[5], 7)};
+    // prod = qh * q, low LW + 1 words
     uint32_t prod[LW + 1];
 #pragma unroll
     for (int w = 0; w <= LW; ++w) prod[w] = 0;
-    {
-        const uint32_t qs[3] = {q0, q1, q2};
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            uint64_t carry = 0;
+    for (int a = 0; a < 3; ++a) {
+        uint64_t carry = 0;
 #pragma unroll
-            for (int l = 0; l + a <= LW; ++l) {
-                const uint32_t ql = l < LW ? q[l] : 0u;
-                const uint64_t cur = uint64_t(prod[l + a]) + uint64_t(qs[a]) * ql + carry;
-                prod[l + a] = uint32_t(cur);
-                carry = cur >> 32;
-            }
+        for (int l = 0; l + a <= LW; ++l) {
+            const uint32_t ql = l < LW ? q[l] : 0u;
+            const uint64_t cur = uint64_t(prod[l + a]) + uint64_t(qs[a]) * ql + carry;
+            prod[l + a] = uint32_t(cur);
+            carry = cur >> 32;
         }
     }
     // r = acc - prod (mod 2^(32 (LW + 1)))
@@ -501,7 +524,7 @@ template <int LW>
 __device__ void crt_coeffs(const ProductDesc& d, const Tables& t, int tile, uint8_t* smem) {
     constexpr int W = LW + kAccExtra;
     const int N = 1 << d.logN;
-    const int logN1 = int(d.logN) > kRowLogMax ? int(d.logN) - kRowLogMax : 0;
+    const int logN1 = int(d.logN) - int(d.logN2);
     const int N2 = N >> logN1;
     const int T = N < kTile ? N : kTile;
     const int C = T >> logN1;
@@ -509,29 +532,24 @@ __device__ void crt_coeffs(const ProductDesc& d, const Tables& t, int tile, uint
     const int j0 = tile * C;
 
     uint64_t* s_res = reinterpret_cast<uint64_t*>(smem);
-    uint8_t* cur = smem + size_t(kTile) * 8 * (k > 16 ? k : 16);
+    uint8_t* cur = smem + smax(size_t(kTile) * 8 * size_t(k), size_t(kTile) * kMaxL * 4);
     uint32_t* s_mq = reinterpret_cast<uint32_t*>(cur);
     cur += size_t(k) * kMqStride * 4;
     uint64_t* s_y = reinterpret_cast<uint64_t*>(cur);
     uint64_t* s_ys = s_y + k;
-    uint64_t* s_p = s_ys + k;
-    cur += size_t(k) * 8 * 3;
-    uint32_t* s_g = reinterpret_cast<uint32_t*>(cur);
-    cur += size_t(k) * 4;
+    cur += size_t(k) * 8 * 2;
     uint32_t* s_negm = reinterpret_cast<uint32_t*>(cur);
     uint32_t* s_q = s_negm + kMqStride;
     uint32_t* s_mu = s_q + kMqStride;
 
     __syncthreads();  // shared memory of a previous item is free
     const QConst* qc = d.qc;
-    for (int w = threadIdx.x; w < k * kMqStride; w += kThreads) s_mq[w] = __ldg(qc->mq + w);
-    for (int w = threadIdx.x; w < k; w += kThreads) {
+    for (int w = threadIdx.x; w < k * kMqStride; w += blockDim.x) s_mq[w] = __ldg(qc->mq + w);
+    for (int w = threadIdx.x; w < k; w += blockDim.x) {
         s_y[w] = __ldg(qc->y + w);
         s_ys[w] = __ldg(qc->ys + w);
-        s_p[w] = __ldg(&t.pc[w].p);
-        s_g[w] = __ldg(&t.pc[w].g);
     }
-    for (int w = threadIdx.x; w < kMqStride; w += kThreads) {
+    for (int w = threadIdx.x; w < kMqStride; w += blockDim.x) {
         s_negm[w] = __ldg(qc->neg_m + w);
         s_q[w] = __ldg(qc->q + w);
     }
@@ -542,36 +560,42 @@ __device__ void crt_coeffs(const ProductDesc& d, const Tables& t, int tile, uint
         case 1: crt_columns<1>(d, t, tile, s_res); break;
         case 2: crt_columns<2>(d, t, tile, s_res); break;
         case 3: crt_columns<3>(d, t, tile, s_res); break;
-        default: crt_columns<4>(d, t, tile, s_res); break;
+        case 4: crt_columns<4>(d, t, tile, s_res); break;
+        default: crt_columns<5>(d, t, tile, s_res); break;
     }
     __syncthreads();
 
     const int tc = threadIdx.x;
     uint32_t r[LW + 1];
     if (tc < T) {
-        uint32_t acc[W];
+        // acc = acc_lo + acc_hi: the lo and hi halves of the limb products run as two independent
+        // carry chains
+        uint32_t acc_lo[W], acc_hi[W];
 #pragma unroll
-        for (int w = 0; w < W; ++w) acc[w] = 0;
+        for (int w = 0; w < W; ++w) acc_lo[w] = acc_hi[w] = 0;
         uint64_t frac = 0;
 #pragma unroll 1
         for (int i = 0; i < k; ++i) {
-            const uint64_t p = s_p[i];
+            const uint64_t p = c_pc[i].p;
             const uint64_t res = s_res[size_t(i) * T + tc];
             const uint64_t v = csub(shoup_lazy(res, s_y[i], s_ys[i], p), p);  // [0, p)
-            frac += (uint64_t(uint32_t(v >> 30)) * s_g[i]) >> 31;              // 2^32 v / p_i
+            frac += (uint64_t(uint32_t(v >> 30)) * c_pc[i].g) >> 31;            // 2^32 v / p_i
             const uint32_t* M = s_mq + i * kMqStride;
-            mac_row<LW, 0, W>(acc, M, uint32_t(v));
-            mac_row<LW, 1, W>(acc, M, uint32_t(v >> 32));
+            const uint32_t v0 = uint32_t(v), v1 = uint32_t(v >> 32);
+            mac_lo<LW, 0, W>(acc_lo, M, v0);
+            mac_hi<LW, 1, W>(acc_hi, M, v0);
+            mac_lo<LW, 1, W>(acc_lo, M, v1);
+            mac_hi<LW, 2, W>(acc_hi, M, v1);
         }
-        // acc += round(sum v_i / p_i) * ((-M) mod q)
+        // acc_lo += round(sum v_i / p_i) * ((-M) mod q)
         const uint32_t kq = uint32_t((frac + (1ull << 31)) >> 32);
-        {
-            uint32_t lo_part[LW];
+        mac_lo<LW, 0, W>(acc_lo, s_negm, kq);
+        mac_hi<LW, 1, W>(acc_hi, s_negm, kq);
+        asm volatile("add.cc.u32 %0, %0, %1;" : "+r"(acc_lo[0]) : "r"(acc_hi[0]));
 #pragma unroll
-            for (int l = 0; l < LW; ++l) lo_part[l] = s_negm[l];
-            mac_row<LW, 0, W>(acc, lo_part, kq);
-        }
-        barrett<LW, W>(acc, s_q, s_mu, int(d.qc->qbits), r);
+        for (int w = 1; w < W - 1; ++w) asm volatile("addc.cc.u32 %0, %0, %1;" : "+r"(acc_lo[w]) : "r"(acc_hi[w]));
+        asm volatile("addc.u32 %0, %0, %1;" : "+r"(acc_lo[W - 1]) : "r"(acc_hi[W - 1]));
+        barrett<LW, W>(acc_lo, s_q, s_mu, int(qc->qbits), r);
     }
     __syncthreads();  // every thread has read s_res; reuse it as output staging
     uint32_t* s_out = reinterpret_cast<uint32_t*>(s_res);
@@ -601,9 +625,9 @@ __device__ void crt_coeffs(const ProductDesc& d, const Tables& t, int tile, uint
         if (((first | size_t(seg)) & 3) == 0) {
             uint4* d4 = reinterpret_cast<uint4*>(dst);
             const uint4* s4 = reinterpret_cast<const uint4*>(src);
-            for (int w = threadIdx.x; w < (seg >> 2); w += kThreads) d4[w] = s4[w];
+            for (int w = threadIdx.x; w < (seg >> 2); w += blockDim.x) d4[w] = s4[w];
         } else {
-            for (int w = threadIdx.x; w < seg; w += kThreads) dst[w] = src[w];
+            for (int w = threadIdx.x; w < seg; w += blockDim.x) dst[w] = src[w];
         }
     }
 }

@@ -40,6 +40,21 @@ C_SYMBOLS = [
     ("nc_plan_stage_ms", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("nc_imad_peak", ctypes.c_int, [ctypes.POINTER(ctypes.c_double)]),
     ("nc_primes", ctypes.c_int, [_u64p, ctypes.c_int]),
+    ("nc_row_variants", ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    ("nc_plan_set_row_config", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("nc_plan_get_row_config", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int)]),
+    ("nc_plan_autotune", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    ("nc_batch_create", ctypes.c_int, [ctypes.POINTER(_vp)]),
+    ("nc_batch_destroy", ctypes.c_int, [_vp]),
+    ("nc_batch_add", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    ("nc_batch_add_cached", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    ("nc_batch_add_forward", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("nc_batch_clear", ctypes.c_int, [_vp]),
+    ("nc_batch_run", ctypes.c_int, [_vp, _vp, ctypes.c_int]),
+    ("nc_batch_synchronize", ctypes.c_int, [_vp]),
+    ("nc_batch_query", ctypes.c_int, [_vp, _u32p, _u32p, _u64p]),
+    ("nc_plan_hat_words", ctypes.c_uint64, [_vp]),
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -137,9 +152,88 @@ class Plan:
     def last_kernel_ms(self) -> float:
         return float(load().nc_plan_last_kernel_ms(self._h))
 
+    @property
+    def row_config(self) -> tuple[int, int, int]:
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(load().nc_plan_get_row_config(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    @row_config.setter
+    def row_config(self, cfg: tuple[int, int, int]) -> None:
+        _check(load().nc_plan_set_row_config(self._h, *map(int, cfg)))
+
+    def autotune(self, reps: int = 5) -> float:
+        """Time every compiled row configuration for this N, keep the fastest; ms per product."""
+        ms = ctypes.c_float()
+        _check(load().nc_plan_autotune(self._h, int(reps), ctypes.byref(ms)))
+        return float(ms.value)
+
+    @property
+    def hat_words(self) -> int:
+        """u64 words of one operand's NTT-domain form (k * N)."""
+        return int(load().nc_plan_hat_words(self._h))
+
     def close(self) -> None:
         if self._h:
             _check(load().nc_plan_destroy(self._h))
+            self._h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def row_variants(log_n: int) -> list[tuple[int, int, int]]:
+    """Compiled row configurations (log_block, log_radix, threads) valid for N = 2^log_n."""
+    n = load().nc_row_variants(int(log_n), None, 0)
+    if n < 0:
+        _check(n)
+    buf = (ctypes.c_int * (3 * max(n, 1)))()
+    got = load().nc_row_variants(int(log_n), buf, n)
+    return [(buf[3 * i], buf[3 * i + 1], buf[3 * i + 2]) for i in range(got)]
+
+
+class Batch:
+    """Many products (any mix of plans) in one persistent launch (nc_batch_*). Device pointers."""
+
+    def __init__(self):
+        self._h = _vp()
+        _check(load().nc_batch_create(ctypes.byref(self._h)))
+
+    def add(self, plan: Plan, d_a: int, d_b: int, d_c: int) -> None:
+        _check(load().nc_batch_add(self._h, plan._h, _vp(d_a), _vp(d_b), _vp(d_c)))
+
+    def add_cached(self, plan: Plan, d_a_hat: int, d_b: int, d_c: int) -> None:
+        _check(load().nc_batch_add_cached(self._h, plan._h, _vp(d_a_hat), _vp(d_b), _vp(d_c)))
+
+    def add_forward(self, plan: Plan, d_a: int, d_a_hat: int) -> None:
+        _check(load().nc_batch_add_forward(self._h, plan._h, _vp(d_a), _vp(d_a_hat)))
+
+    def clear(self) -> None:
+        _check(load().nc_batch_clear(self._h))
+
+    def run(self, stream: int = 0, use_graph: bool = True) -> None:
+        _check(load().nc_batch_run(self._h, _vp(stream or None), int(use_graph)))
+
+    def synchronize(self) -> None:
+        _check(load().nc_batch_synchronize(self._h))
+
+    def query(self) -> dict:
+        n, c, s = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
+        _check(load().nc_batch_query(self._h, ctypes.byref(n), ctypes.byref(c), ctypes.byref(s)))
+        return {"products": n.value, "ctas": c.value, "scratch_bytes": s.value}
+
+    def close(self) -> None:
+        if self._h:
+            _check(load().nc_batch_destroy(self._h))
             self._h = _vp()
 
     def __enter__(self):

@@ -79,6 +79,49 @@ int nc_imad_peak(double* ops_per_second);
 /* Residue primes of the fixed set (p = 2^62 - m, p = 1 mod 2^17), first `count` of 48. */
 int nc_primes(uint64_t* out, int count);
 
+/* ------------------------------------------------------------------ tuning */
+
+/* Row-stage tiling of the plan's plain path: row blocks of 2^log_block residues, 2^log_radix
+   residues per thread per register pass, CTAs of `threads` threads. nc_row_variants lists the
+   compiled configurations valid for ring degree 2^log_n as triples (log_block, log_radix,
+   threads); it returns how many it wrote, or a negative status. */
+int nc_row_variants(uint32_t log_n, int* triples, int max_variants);
+int nc_plan_set_row_config(nc_plan* plan, int log_block, int log_radix, int threads);
+int nc_plan_get_row_config(const nc_plan* plan, int* log_block, int* log_radix, int* threads);
+
+/* Autotuner: times every compiled row configuration for the plan's N on the device (`reps`
+   products each), keeps the fastest for this plan and for later plans of the same (N, L) in
+   this process, and writes its milliseconds per product to best_ms (may be NULL). */
+int nc_plan_autotune(nc_plan* plan, int reps, float* best_ms);
+
+/* ------------------------------------------------------------------ batches
+ *
+ * A batch runs many products, of any mix of N and q (one plan each), in ONE persistent kernel
+ * launch: per-(prime, row block) and per-tile work items in a global queue, dependency
+ * counters per product, bounded waits. The counter reset and the launch are captured into a
+ * CUDA graph and replayed while the batch keeps its shape. Device buffers are 16-byte aligned
+ * and must stay valid until the batch has run. */
+
+typedef struct nc_batch nc_batch;
+
+int nc_batch_create(nc_batch** out);
+int nc_batch_destroy(nc_batch* batch);
+/* c = a * b (device buffers, plan's N x L limbs). */
+int nc_batch_add(nc_batch* batch, nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c);
+/* c = a * b with a given in the NTT domain (nc_plan_hat_words u64 words, from nc_batch_add_forward). */
+int nc_batch_add_cached(nc_batch* batch, nc_plan* plan, const uint64_t* d_a_hat, const uint32_t* d_b, uint32_t* d_c);
+/* a_hat = the NTT-domain form of a, for reuse as a cached operand. */
+int nc_batch_add_forward(nc_batch* batch, nc_plan* plan, const uint32_t* d_a, uint64_t* d_a_hat);
+int nc_batch_clear(nc_batch* batch);
+/* Enqueue every product on `stream` (0: default stream); use_graph replays a captured graph. */
+int nc_batch_run(nc_batch* batch, void* stream, int use_graph);
+/* Waits for the last run; NC_ETIMEOUT if a dependency wait gave up. */
+int nc_batch_synchronize(nc_batch* batch);
+/* Products, persistent CTAs of the last run, bytes of residue scratch held. Pointers may be NULL. */
+int nc_batch_query(const nc_batch* batch, uint32_t* products, uint32_t* ctas, uint64_t* scratch_bytes);
+/* u64 words of the NTT-domain form of one operand of this plan (k * N). */
+uint64_t nc_plan_hat_words(const nc_plan* plan);
+
 #ifdef __cplusplus
 }
 #endif

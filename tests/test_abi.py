@@ -102,3 +102,22 @@ def test_prime_set():
         assert p < (1 << 62) and p % (1 << 17) == 1
         assert (1 << 62) - p < (1 << 28)
         assert cases.is_probable_prime(p, 16, rng)
+
+
+def test_row_variants_listed_without_gpu():
+    for log_n in range(1, 17):
+        v = nc.row_variants(log_n)
+        assert v, log_n
+        for blk, radix, threads in v:
+            assert 1 <= blk <= min(log_n, 13) and log_n - blk <= 5
+            assert radix in (3, 4) and threads in (256, 512)
+    assert (12, 4, 256) in nc.row_variants(16)
+    assert nc.load().nc_row_variants(17, None, 0) == nc.NC_EINVAL
+
+
+def test_batch_entry_points_reject_nulls():
+    lib = nc.load()
+    assert lib.nc_batch_add(None, None, None, None, None) == nc.NC_EINVAL
+    assert lib.nc_batch_run(None, None, 1) == nc.NC_EINVAL
+    assert lib.nc_batch_destroy(None) == nc.NC_OK
+    assert lib.nc_plan_hat_words(None) == 0
