@@ -12,9 +12,7 @@
 #include "hostmath.h"
 #include "kernels.h"
 
-struct nc_plan {
-    nc::Plan* p;
-};
+#include "handles.h"
 
 namespace {
 
@@ -39,6 +37,8 @@ int guarded(F&& f) {
 }
 
 }  // namespace
+
+void nc::set_last_error(const std::string& msg) { g_last_error = msg; }
 
 extern "C" {
 

@@ -33,6 +33,7 @@ C_SYMBOLS = [
     ("nc_plan_destroy", ctypes.c_int, [_vp]),
     ("nc_multiply", ctypes.c_int, [_vp, _u32p, _u32p, _u32p]),
     ("nc_multiply_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    ("nc_multiply_device_noalloc", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     ("nc_plan_synchronize", ctypes.c_int, [_vp]),
     ("nc_plan_query", ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _u32p]),
     ("nc_plan_last_kernel_ms", ctypes.c_float, [_vp]),
@@ -136,6 +137,12 @@ class Plan:
     def multiply_device(self, d_a: int, d_b: int, d_c: int, stream: int = 0) -> None:
         """Device pointers (e.g. torch tensor .data_ptr()), enqueued on `stream` (0: default stream)."""
         _check(load().nc_multiply_device(self._h, _vp(d_a), _vp(d_b), _vp(d_c), _vp(stream or None)))
+
+    def multiply_device_noalloc(self, d_a: int, d_b: int, d_c: int, stream: int = 0) -> None:
+        """Like multiply_device, but allocates nothing: for callers that must not allocate device
+        memory at call time. Its residue scratch is one 8 MiB array inside the library shared by
+        all calls (so overlapping calls race); limit k * N <= 2^19 (N <= 16384 at an 868-bit q)."""
+        _check(load().nc_multiply_device_noalloc(self._h, _vp(d_a), _vp(d_b), _vp(d_c), _vp(stream or None)))
 
     def synchronize(self) -> None:
         _check(load().nc_plan_synchronize(self._h))

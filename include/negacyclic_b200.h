@@ -56,6 +56,18 @@ int nc_multiply(nc_plan* plan, const uint32_t* a, const uint32_t* b, uint32_t* c
    residues, so calls on one plan must not overlap on the device. */
 int nc_multiply_device(nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream);
 
+/* Same product as nc_multiply_device, for callers that must not allocate device memory when
+   they call it (device memory owned by another framework's pool, latency-critical loops where
+   cudaMalloc's implicit synchronisation is unacceptable, services that allocate only at
+   start-up). It allocates nothing: the residue scratch is a fixed 8 MiB array inside the library
+   (held on every GPU that loads it until exit) instead of the plan's own scratch. Limit:
+   k * N <= 2^19 (N <= 16384 at an 868-bit q); larger products return NC_EINVAL. All calls share
+   that array, so calls that overlap on the GPU race; nothing in it needs to start at zero. The
+   first call on a device looks up the array's device address and should come before any stream
+   capture on that device. This entry point has no counterpart in the reference. */
+int nc_multiply_device_noalloc(const nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
+                               void* stream);
+
 /* Waits for the plan's own stream (the one nc_multiply uses). */
 int nc_plan_synchronize(nc_plan* plan);
 
