@@ -34,8 +34,25 @@ LIB_SOURCES = ["hostmath.cpp", "k_dec.cu", "k_row.cu", "k_crt.cu", "k_batch.cu",
 RUNNER_SOURCES = ["runner.cpp"]
 
 
-def _headers() -> list[Path]:
-    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
+def _headers(src: Path | None = None) -> list[Path]:
+    """Headers `src` includes, transitively (quoted includes found in csrc/ or include/)."""
+    if src is None:
+        return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
+    seen: set[Path] = set()
+    todo = [src]
+    while todo:
+        f = todo.pop()
+        for line in f.read_text(errors="replace").splitlines():
+            line = line.strip()
+            if not line.startswith("#include \""):
+                continue
+            name = line.split('"')[1]
+            for d in (CSRC, INCLUDE):
+                h = d / name
+                if h.exists() and h not in seen:
+                    seen.add(h)
+                    todo.append(h)
+    return sorted(seen)
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:
@@ -47,7 +64,7 @@ def _stale(target: Path, deps: list[Path]) -> bool:
 
 def _compile(src: Path, verbose: bool) -> Path:
     obj = OBJ / (src.name + ".o")
-    if not _stale(obj, [src] + _headers()):
+    if not _stale(obj, [src] + _headers(src)):
         return obj
     cmd = [NVCC, *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cu" and verbose:

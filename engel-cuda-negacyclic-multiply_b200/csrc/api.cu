@@ -10,9 +10,9 @@
 #include "batch.h"
 #include "engine.h"
 #include "hostmath.h"
-#include "kernels.h"
-
 #include "handles.h"
+#include "kernels.h"
+#include "server.h"
 
 namespace {
 
@@ -289,6 +289,86 @@ int nc_batch_query(const nc_batch* batch, uint32_t* products, uint32_t* ctas, ui
         if (products) *products = uint32_t(batch->b->size());
         if (ctas) *ctas = uint32_t(batch->b->ctas());
         if (scratch_bytes) *scratch_bytes = uint64_t(batch->b->scratch_bytes());
+    });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ serving
+
+struct nc_server {
+    nc::Server* s;
+};
+
+extern "C" {
+
+int nc_server_create(uint64_t hbm_budget_bytes, uint64_t staging_bytes, int max_batch, int streams, nc_server** out) {
+    return guarded([&] {
+        if (!out) throw nc::Error(nc::kEInval, "out is null");
+        *out = nullptr;
+        auto* s = new nc::Server(nc::current_device(), size_t(hbm_budget_bytes), size_t(staging_bytes), max_batch,
+                                 streams);
+        *out = new nc_server{s};
+    });
+}
+
+int nc_server_destroy(nc_server* server) {
+    return guarded([&] {
+        if (!server) return;
+        delete server->s;
+        delete server;
+    });
+}
+
+int nc_server_register_operand(nc_server* server, nc_plan* plan, const uint32_t* a, int* operand_id) {
+    return guarded([&] {
+        if (!server || !plan || !operand_id) throw nc::Error(nc::kEInval, "null argument");
+        *operand_id = server->s->register_operand(plan->p, a);
+    });
+}
+
+int nc_server_release_operand(nc_server* server, int operand_id) {
+    return guarded([&] {
+        if (!server) throw nc::Error(nc::kEInval, "null server");
+        server->s->release_operand(operand_id);
+    });
+}
+
+int nc_server_submit(nc_server* server, nc_plan* plan, const uint32_t* a, int operand_id, const uint32_t* b,
+                     uint64_t* request_id) {
+    return guarded([&] {
+        if (!server || !plan || !request_id) throw nc::Error(nc::kEInval, "null argument");
+        *request_id = server->s->submit(plan->p, a, operand_id, b);
+    });
+}
+
+int nc_server_poll(nc_server* server, uint64_t request_id) {
+    int r = 0;
+    const int st = guarded([&] {
+        if (!server) throw nc::Error(nc::kEInval, "null server");
+        r = server->s->done(request_id) ? 1 : 0;
+    });
+    return st == NC_OK ? r : st;
+}
+
+int nc_server_wait(nc_server* server, uint64_t request_id, uint32_t* c, double* latency_ms) {
+    return guarded([&] {
+        if (!server) throw nc::Error(nc::kEInval, "null server");
+        const double ms = server->s->wait(request_id, c);
+        if (latency_ms) *latency_ms = ms;
+    });
+}
+
+int nc_server_stats(nc_server* server, double* p50_ms, double* p99_ms, uint64_t* completed, double* products_per_s,
+                    uint64_t* hbm_in_use, uint64_t* batches) {
+    return guarded([&] {
+        if (!server) throw nc::Error(nc::kEInval, "null server");
+        size_t in_use = 0;
+        uint64_t done = 0, b = 0;
+        server->s->stats(p50_ms, p99_ms, &done, products_per_s, &in_use, &b);
+        if (completed) *completed = done;
+        if (hbm_in_use) *hbm_in_use = in_use;
+        if (batches) *batches = b;
     });
 }
 

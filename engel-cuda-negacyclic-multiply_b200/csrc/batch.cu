@@ -26,10 +26,19 @@ void ensure(T** p, size_t* cap, size_t count, const char* what) {
 
 }  // namespace
 
-Batch::Batch(int device) : device_(device) { tables_ = acquire_tables(device); }
+Batch::Batch(int device) : device_(device) {
+    tables_ = acquire_tables(device);
+    const cudaError_t e = cudaEventCreateWithFlags(&done_, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        release_tables(tables_);
+        check(e, "batch event");
+    }
+}
 
 Batch::~Batch() {
-    if (last_stream_) cudaStreamSynchronize(last_stream_);
+    // wait on the batch's own event (never on the caller's stream, which may be gone)
+    if (ran_) cudaEventSynchronize(done_);
+    cudaEventDestroy(done_);
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
     cudaFree(d_products_);
@@ -40,7 +49,7 @@ Batch::~Batch() {
 }
 
 void Batch::add(Plan* plan, uint32_t mode, const uint32_t* a, const uint32_t* b, uint32_t* c, const uint64_t* a_hat,
-                uint64_t* hat_out) {
+                uint64_t* hat_out, uint64_t* scratch) {
     if (!plan) throw Error(kEInval, "null plan");
     if (plan->device != device_) throw Error(kEInval, "the plan lives on another device");
     if (mode > kModeForward) throw Error(kEInval, "unknown product mode");
@@ -53,7 +62,8 @@ void Batch::add(Plan* plan, uint32_t mode, const uint32_t* a, const uint32_t* b,
                             reinterpret_cast<uintptr_t>(hat_out);
     if (align & 15) throw Error(kEInval, "device buffers must be 16-byte aligned");
     if (entries_.size() >= (size_t(1) << 28)) throw Error(kEInval, "batch too large");
-    entries_.push_back(Entry{plan, mode, a, b, c, a_hat, hat_out});
+    if (reinterpret_cast<uintptr_t>(scratch) & 255) throw Error(kEInval, "scratch must be 256-byte aligned");
+    entries_.push_back(Entry{plan, mode, a, b, c, a_hat, hat_out, scratch});
     dirty_ = true;
 }
 
@@ -63,6 +73,8 @@ void Batch::clear() {
 }
 
 void Batch::finalize() {
+    // the previous run may still read the device-side product and item tables
+    if (ran_) check(cudaEventSynchronize(done_), "batch");
     const size_t n = entries_.size();
     std::vector<BatchProduct> prods(n);
     std::vector<uint64_t> shape;
@@ -70,7 +82,7 @@ void Batch::finalize() {
     int kmax = 1;
     for (size_t p = 0; p < n; ++p) {
         const Plan* pl = entries_[p].plan;
-        scratch += 2 * round_up(size_t(pl->k) * pl->N * sizeof(uint64_t), 256);
+        if (!entries_[p].scratch) scratch += 2 * round_up(size_t(pl->k) * pl->N * sizeof(uint64_t), 256);
         kmax = std::max(kmax, pl->k);
     }
     if (scratch > scratch_bytes_) {
@@ -94,9 +106,14 @@ void Batch::finalize() {
         d.a_hat = e.a_hat;
         d.hat_out = e.hat_out;
         const size_t res = round_up(size_t(pl->k) * pl->N * sizeof(uint64_t), 256);
-        d.ra = reinterpret_cast<uint64_t*>(base + off);
-        d.rb = reinterpret_cast<uint64_t*>(base + off + res);
-        off += 2 * res;
+        if (e.scratch) {
+            d.ra = e.scratch;
+            d.rb = e.scratch + res / sizeof(uint64_t);
+        } else {
+            d.ra = reinterpret_cast<uint64_t*>(base + off);
+            d.rb = reinterpret_cast<uint64_t*>(base + off + res);
+            off += 2 * res;
+        }
         BatchProduct& bp = prods[p];
         bp.d = d;
         bp.tiles = uint32_t(g.tiles);
@@ -152,10 +169,11 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
     args.error = d_state_ + 2 * n + 1;
     args.tables = tables_->view();
     const size_t state_bytes = (2 * n + 2) * sizeof(uint32_t);
-    last_stream_ = stream;
     if (!use_graph) {
         check(cudaMemsetAsync(d_state_, 0, state_bytes, stream), "batch reset");
         check(launch_persistent(args, ctas_, smem_, stream), "persistent launch");
+        check(cudaEventRecord(done_, stream), "batch event");
+        ran_ = true;
         return;
     }
     if (!exec_) {
@@ -172,11 +190,13 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
         check(cudaGraphInstantiate(&exec_, graph_, 0), "graph instantiate");
     }
     check(cudaGraphLaunch(exec_, stream), "graph launch");
+    check(cudaEventRecord(done_, stream), "batch event");
+    ran_ = true;
 }
 
 void Batch::synchronize() {
-    if (!last_stream_ && entries_.empty()) return;
-    check(cudaStreamSynchronize(last_stream_), "batch");
+    if (!ran_) return;
+    check(cudaEventSynchronize(done_), "batch");
     if (entries_.empty()) return;
     uint32_t err = 0;
     check(cudaMemcpy(&err, d_state_ + 2 * entries_.size() + 1, sizeof(err), cudaMemcpyDeviceToHost), "batch status");

@@ -22,8 +22,10 @@ class Batch {
 
     // mode: kModeProduct (a, b -> c), kModeCachedA (a_hat in the NTT domain, b -> c),
     //       kModeForward (a -> a_hat: the NTT-domain form of an operand, for caching).
+    // `scratch` (optional): 2 * k * N u64 of residue scratch owned by the caller; without it the
+    // product takes its scratch from the batch's own arena.
     void add(Plan* plan, uint32_t mode, const uint32_t* a, const uint32_t* b, uint32_t* c, const uint64_t* a_hat,
-             uint64_t* hat_out);
+             uint64_t* hat_out, uint64_t* scratch = nullptr);
     void clear();
     size_t size() const { return entries_.size(); }
     // Enqueue the whole batch on `stream` (graph replay when `use_graph`).
@@ -43,6 +45,7 @@ class Batch {
         uint32_t* c;
         const uint64_t* a_hat;
         uint64_t* hat_out;
+        uint64_t* scratch;
     };
     void finalize();
     int device_;
@@ -62,7 +65,8 @@ class Batch {
     size_t smem_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
-    cudaStream_t last_stream_ = nullptr;
+    cudaEvent_t done_ = nullptr;  // recorded after every run
+    bool ran_ = false;
     bool dirty_ = true;
 };
 

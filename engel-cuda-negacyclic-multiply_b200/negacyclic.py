@@ -56,6 +56,16 @@ C_SYMBOLS = [
     ("nc_batch_synchronize", ctypes.c_int, [_vp]),
     ("nc_batch_query", ctypes.c_int, [_vp, _u32p, _u32p, _u64p]),
     ("nc_plan_hat_words", ctypes.c_uint64, [_vp]),
+    ("nc_server_create", ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(_vp)]),
+    ("nc_server_destroy", ctypes.c_int, [_vp]),
+    ("nc_server_register_operand", ctypes.c_int, [_vp, _vp, _u32p, ctypes.POINTER(ctypes.c_int)]),
+    ("nc_server_release_operand", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nc_server_submit", ctypes.c_int, [_vp, _vp, _u32p, ctypes.c_int, _u32p, _u64p]),
+    ("nc_server_poll", ctypes.c_int, [_vp, ctypes.c_uint64]),
+    ("nc_server_wait", ctypes.c_int, [_vp, ctypes.c_uint64, _u32p, ctypes.POINTER(ctypes.c_double)]),
+    ("nc_server_stats", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _u64p,
+                                       ctypes.POINTER(ctypes.c_double), _u64p, _u64p]),
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -241,6 +251,71 @@ class Batch:
     def close(self) -> None:
         if self._h:
             _check(load().nc_batch_destroy(self._h))
+            self._h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching server (nc_server_*): host operands in, products out."""
+
+    def __init__(self, hbm_budget: int = 1 << 30, staging: int = 1 << 28, max_batch: int = 64, streams: int = 2):
+        self._h = _vp()
+        _check(load().nc_server_create(int(hbm_budget), int(staging), int(max_batch), int(streams),
+                                       ctypes.byref(self._h)))
+
+    def register_operand(self, plan: Plan, a: np.ndarray) -> int:
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        oid = ctypes.c_int()
+        _check(load().nc_server_register_operand(self._h, plan._h, _u32(a), ctypes.byref(oid)))
+        return oid.value
+
+    def release_operand(self, oid: int) -> None:
+        _check(load().nc_server_release_operand(self._h, int(oid)))
+
+    def submit(self, plan: Plan, a: np.ndarray | None, b: np.ndarray, operand: int = -1) -> int:
+        b = np.ascontiguousarray(b, dtype=np.uint32)
+        a_ptr = None
+        if a is not None:
+            a = np.ascontiguousarray(a, dtype=np.uint32)
+            a_ptr = _u32(a)
+        rid = ctypes.c_uint64()
+        _check(load().nc_server_submit(self._h, plan._h, a_ptr, int(operand), _u32(b), ctypes.byref(rid)))
+        return rid.value
+
+    def poll(self, rid: int) -> bool:
+        st = load().nc_server_poll(self._h, int(rid))
+        if st < 0:
+            _check(st)
+        return st == 1
+
+    def wait(self, rid: int, plan: Plan) -> tuple[np.ndarray, float]:
+        c = np.empty((plan.N, plan.L), dtype=np.uint32)
+        ms = ctypes.c_double()
+        _check(load().nc_server_wait(self._h, int(rid), _u32(c), ctypes.byref(ms)))
+        return c, ms.value
+
+    def stats(self) -> dict:
+        p50, p99, pps = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        done, hbm, batches = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(load().nc_server_stats(self._h, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(done),
+                                      ctypes.byref(pps), ctypes.byref(hbm), ctypes.byref(batches)))
+        return {"p50_ms": p50.value, "p99_ms": p99.value, "completed": done.value, "products_per_s": pps.value,
+                "hbm_in_use": hbm.value, "batches": batches.value}
+
+    def close(self) -> None:
+        if self._h:
+            _check(load().nc_server_destroy(self._h))
             self._h = _vp()
 
     def __enter__(self):

@@ -134,6 +134,33 @@ int nc_batch_query(const nc_batch* batch, uint32_t* products, uint32_t* ctas, ui
 /* u64 words of the NTT-domain form of one operand of this plan (k * N). */
 uint64_t nc_plan_hat_words(const nc_plan* plan);
 
+/* ------------------------------------------------------------------ serving
+ *
+ * Continuous batching. nc_server_submit copies host operands into pinned staging and returns a
+ * request id (it blocks while staging is full). A scheduler thread admits queued requests in
+ * arrival order while the HBM budget holds them (operands, product and residue scratch), runs
+ * everything admitted as one persistent batch on the next free stream, and keeps admitting new
+ * requests into further batches while earlier ones run, so their work overlaps on the device.
+ * Operands registered with nc_server_register_operand stay resident in their NTT-domain form;
+ * requests that name one (a = NULL, operand_id >= 0) skip its transform. nc_server_wait returns
+ * the product and the request's latency from submit to result in pinned host memory. */
+
+typedef struct nc_server nc_server;
+
+int nc_server_create(uint64_t hbm_budget_bytes, uint64_t staging_bytes, int max_batch, int streams, nc_server** out);
+int nc_server_destroy(nc_server* server);
+int nc_server_register_operand(nc_server* server, nc_plan* plan, const uint32_t* a, int* operand_id);
+int nc_server_release_operand(nc_server* server, int operand_id);
+int nc_server_submit(nc_server* server, nc_plan* plan, const uint32_t* a, int operand_id, const uint32_t* b,
+                     uint64_t* request_id);
+/* 1 when the request is finished (nc_server_wait returns at once), 0 while pending. */
+int nc_server_poll(nc_server* server, uint64_t request_id);
+int nc_server_wait(nc_server* server, uint64_t request_id, uint32_t* c, double* latency_ms);
+/* Latency percentiles over completed requests, their count, completed products per second
+   since the first submit, device bytes in use, batches launched. Pointers may be NULL. */
+int nc_server_stats(nc_server* server, double* p50_ms, double* p99_ms, uint64_t* completed, double* products_per_s,
+                    uint64_t* hbm_in_use, uint64_t* batches);
+
 #ifdef __cplusplus
 }
 #endif
