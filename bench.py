@@ -29,6 +29,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import queue
 import shutil
 import statistics
 import subprocess
@@ -43,11 +44,16 @@ sys.path.insert(0, str(PKG))
 
 METRIC = "products/s at N=2^16, 868-bit q, bit-exact: batched vs plain; serve p50/p99 ms"
 N_MAIN, BITS, SEED, EDGE = 65536, 868, 20261203, 0.01
+MIX_SEED = 4242
 WORKLOAD = "single large product: N=65536, L=28, seeded 868-bit prime q, 1% edge coefficients"
 FLUSH_BYTES = 256 << 20
 RUNNER = PKG / "bin" / "solution"
 REF_BINARY = ROOT / "oracle" / "_ref" / "solution_patched"
 TRAFFIC_FILE = ROOT / "profiles" / "traffic.json"
+
+
+def log(msg: str) -> None:
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
 
 
 def parse_args():
@@ -58,6 +64,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched / uneven / serving sections")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.steps = max(a.steps, 1)
@@ -225,12 +232,19 @@ def dist_setup(args):
 
 def ours(args) -> dict | None:
     import numpy as np
-    import torch
 
     import cases
-    import negacyclic as nc
 
     world, rank, local = dist_setup(args)
+    forms = world == 1 and not args.no_forms
+    mix = None
+    if forms:  # seeded primes of the uneven mix, found before this process touches CUDA
+        mix = cases.uneven_mix(256, seed=MIX_SEED, processes=min(16, os.cpu_count() or 1))
+
+    import torch
+
+    import negacyclic as nc
+
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     pg = None
@@ -370,11 +384,215 @@ def ours(args) -> dict | None:
                          "h2d_bytes_per_step": 2 * N * L * 4, "d2h_bytes_per_step": N * L * 4,
                          "ms_p50": 1e3 * statistics.median(secs), "init_s": init_s,
                          "via": "fherma_run in the library's harness runner (pageable std::vector in/out)"}
+    if forms:
+        log("batched N=65536")
+        result["batched_n65536"] = batched_same_shape(dev, case.q, 65536, 16, args)
+        log("batched 64 x N=16384")
+        result["batched_c3"] = batched_same_shape(dev, case.q, 16384, 64, args)
+        log("uneven batch")
+        result["uneven_c4"] = uneven_batch(dev, mix, args)
+        log("serving")
+        result["serve_c5"] = serving(dev, mix, args)
+        log("forms done")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(case)
     if pg:
         pg.destroy_process_group()
     return result if rank == 0 else None
+
+
+# ----------------------------------------------------------------------------- batched forms
+
+
+def _event_ms(fn, warmup: int, reps: int) -> float:
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def batched_same_shape(dev, q: int, N: int, count: int, args) -> dict:
+    """`count` products of one (N, q): one persistent launch replayed from a CUDA graph, against
+    the same products as back-to-back plain per-call launches. Operands (> L2) stay in HBM."""
+    import numpy as np
+    import torch
+
+    import cases
+    import negacyclic as nc
+
+    L = (BITS + 31) // 32
+    ql = cases.limbs_of(q, L)
+    rng = np.random.default_rng(N + count)
+    a = [torch.from_numpy(cases.coeffs(q, N, L, 9000 + i).view(np.int32)).to(dev) for i in range(min(count, 8))]
+    b = [torch.from_numpy(cases.coeffs(q, N, L, 9100 + i).view(np.int32)).to(dev) for i in range(min(count, 8))]
+    ops = [(a[i % len(a)], b[(i * 5 + 3) % len(b)]) for i in range(count)]
+    outs_b = [torch.empty_like(a[0]) for _ in range(count)]
+    outs_p = [torch.empty_like(a[0]) for _ in range(count)]
+    del rng
+    with nc.Plan(N, ql) as plan, nc.Batch() as batch:
+        plan.autotune(reps=2)
+        for (x, y), z in zip(ops, outs_b):
+            batch.add(plan, x.data_ptr(), y.data_ptr(), z.data_ptr())
+
+        def run_batch():
+            batch.run(0, True)
+
+        def run_plain():
+            for (x, y), z in zip(ops, outs_p):
+                plan.multiply_device(x.data_ptr(), y.data_ptr(), z.data_ptr(), 0)
+
+        ms_batch = _event_ms(run_batch, 2, 5)
+        batch.synchronize()
+        ms_plain = _event_ms(run_plain, 2, 5)
+        exact = all(torch.equal(p, q_) for p, q_ in zip(outs_b, outs_p))
+        info = batch.query()
+    if not exact:
+        raise RuntimeError(f"batched and plain products differ at N={N}")
+    return {"products": count, "N": N, "q_bits": BITS,
+            "batched": {"value": count / (ms_batch * 1e-3), "unit": "products/s", "ms_per_launch": ms_batch,
+                        "ctas": info["ctas"], "gpu_launches_per_batch": 1,
+                        "form": "one persistent launch, CUDA graph replay"},
+            "plain": {"value": count / (ms_plain * 1e-3), "unit": "products/s",
+                      "gpu_launches_per_batch": 3 * count, "form": "3 launches per product, back to back"},
+            "speedup": ms_plain / ms_batch, "bit_exact_vs_plain": exact}
+
+
+def uneven_batch(dev, mix, args) -> dict:
+    """The 256-product uneven mix (N log-uniform 2^10..2^16, 434- and 868-bit seeded q) in one
+    persistent launch, against per-product plain launches of the same products."""
+    import numpy as np
+    import torch
+
+    import cases
+    import negacyclic as nc
+
+    plans, bufs = [], []
+    for i, (N, bits, q) in enumerate(mix):
+        L = (bits + 31) // 32
+        p = nc.Plan(N, cases.limbs_of(q, L))
+        x = torch.from_numpy(cases.coeffs(q, N, L, 11000 + i).view(np.int32)).to(dev)
+        y = torch.from_numpy(cases.coeffs(q, N, L, 12000 + i).view(np.int32)).to(dev)
+        plans.append(p)
+        bufs.append((x, y, torch.empty_like(x), torch.empty_like(x)))
+    try:
+        with nc.Batch() as batch:
+            for p, (x, y, z, _) in zip(plans, bufs):
+                batch.add(p, x.data_ptr(), y.data_ptr(), z.data_ptr())
+            ms_batch = _event_ms(lambda: batch.run(0, True), 2, 5)
+            batch.synchronize()
+
+            def plain():
+                for p, (x, y, _, w) in zip(plans, bufs):
+                    p.multiply_device(x.data_ptr(), y.data_ptr(), w.data_ptr(), 0)
+
+            ms_plain = _event_ms(plain, 1, 3)
+            exact = all(torch.equal(z, w) for _, _, z, w in bufs)
+            info = batch.query()
+    finally:
+        for p in plans:
+            p.close()
+    if not exact:
+        raise RuntimeError("uneven batch differs from plain products")
+    total_imad = 0.0
+    for N, bits, _ in mix:
+        L = (bits + 31) // 32
+        k = 29 if bits > 600 else 15
+        total_imad += sum(stage_work(k, N, L))
+    return {"products": len(mix), "mix": "N log-uniform 2^10..2^16, q 434- or 868-bit (seeded per product)",
+            "batched": {"value": len(mix) / (ms_batch * 1e-3), "unit": "products/s", "ms_per_launch": ms_batch,
+                        "ctas": info["ctas"], "imad_alg_rate_gops": total_imad / (ms_batch * 1e-3) / 1e9},
+            "plain": {"value": len(mix) / (ms_plain * 1e-3), "unit": "products/s", "ms": ms_plain},
+            "speedup": ms_plain / ms_batch, "bit_exact_vs_plain": exact}
+
+
+def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
+    """Poisson arrivals of the uneven mix at each rate; 30% of requests reuse one of 8 registered
+    operands (NTT form cached on the device); admission by a 40 GB HBM budget. The same arrival
+    schedule is also served by the plain per-call form (one worker, fherma_run-style host calls)."""
+    import random
+    import threading
+
+    import numpy as np
+
+    import cases
+    import negacyclic as nc
+
+    rng = random.Random(MIX_SEED)
+    sub = mix[:64]  # 64 distinct (N, q) plans serve the requests
+    plans = []
+    for N, bits, q in sub:
+        L = (bits + 31) // 32
+        plans.append((nc.Plan(N, cases.limbs_of(q, L)), q, L))
+    host = [(cases.coeffs(q, p.N, L, 13000 + i), cases.coeffs(q, p.N, L, 14000 + i)) for i, (p, q, L) in
+            enumerate(plans)]
+    out = {"budget_bytes": 40 << 30, "requests_per_rate": requests, "reuse_fraction": 0.3, "rates": []}
+    try:
+        for rate in rates:
+            sched = []
+            t = 0.0
+            for _ in range(requests):
+                t += rng.expovariate(rate)
+                pi = rng.randrange(len(plans))
+                sched.append((t, pi, rng.random() < 0.3 and pi < 8))
+            row = {"rate_per_s": rate}
+            with nc.Server(hbm_budget=40 << 30, staging=2 << 30, max_batch=64, streams=3) as srv:
+                opids = {i: srv.register_operand(plans[i][0], host[i][0]) for i in range(8)}
+                clients = 8  # independent Poisson clients (their superposition is Poisson at `rate`)
+                t0 = time.perf_counter()
+
+                def producer(c, pending):
+                    for ta, pi, reuse in sched[c::clients]:
+                        while time.perf_counter() - t0 < ta:
+                            time.sleep(0)
+                        p = plans[pi][0]
+                        a, b = host[pi]
+                        pending.put((pi, srv.submit(p, None if reuse else a, b, operand=opids[pi] if reuse else -1)))
+                    pending.put(None)
+
+                def consumer(pending):  # each client collects its results as they come
+                    while (item := pending.get()) is not None:
+                        srv.wait(item[1], plans[item[0]][0])
+
+                threads = []
+                for c in range(clients):
+                    qq = queue.Queue()
+                    threads += [threading.Thread(target=producer, args=(c, qq)), threading.Thread(target=consumer, args=(qq,))]
+                for th in threads:
+                    th.start()
+                for th in threads:
+                    th.join()
+                st = srv.stats()
+            row["server"] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "products_per_s": st["products_per_s"],
+                             "batches": st["batches"]}
+            # plain per-call form on the same schedule: one worker, host operands in and out
+            if rate == rates[0]:
+                for (p, _, _), (a, b) in zip(plans, host):
+                    p.multiply(a, b)  # first use allocates each plan's staging: keep it out of the timing
+            lat = []
+            t0 = time.perf_counter()
+            for ta, pi, _ in sched:
+                while time.perf_counter() - t0 < ta:
+                    pass
+                p = plans[pi][0]
+                a, b = host[pi]
+                p.multiply(a, b)
+                lat.append(1e3 * (time.perf_counter() - t0 - ta))
+            wall = time.perf_counter() - t0
+            row["plain_per_call"] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                                     "products_per_s": requests / wall}
+            out["rates"].append(row)
+    finally:
+        for p, _, _ in plans:
+            p.close()
+    return out
 
 
 def _hbm_peak():

@@ -59,6 +59,66 @@ def gen_prime(bits: int, seed: int, rounds: int = 40) -> int:
             return x
 
 
+def _primorial(limit: int) -> int:
+    sieve = bytearray([1]) * limit
+    sieve[0:2] = b"\x00\x00"
+    for i in range(2, int(limit ** 0.5) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = bytearray(len(sieve[i * i::i]))
+    out = 1
+    for i, s in enumerate(sieve):
+        if s:
+            out *= i
+    return out
+
+
+_PRIMORIAL = None
+
+
+def gen_prime_fast(bits: int, seed: int, rounds: int = 40) -> int:
+    """Seeded `bits`-bit prime (top bit set, Miller-Rabin `rounds` rounds with seeded bases).
+    Candidates sharing a factor below 10000 are dropped by one gcd before any Miller-Rabin
+    round, so it is several times faster than gen_prime; it yields different primes for the
+    same seed (its own seeded sequence)."""
+    global _PRIMORIAL
+    import math
+
+    if _PRIMORIAL is None:
+        _PRIMORIAL = _primorial(10000)
+    rng = random.Random(seed)
+    while True:
+        x = rng.getrandbits(bits) | (1 << (bits - 1)) | 1
+        if math.gcd(x, _PRIMORIAL) != 1:
+            continue
+        if is_probable_prime(x, rounds, rng):
+            return x
+
+
+def _prime_job(args):
+    return gen_prime_fast(*args)
+
+
+def uneven_mix(count: int, seed: int, log_n=(10, 16), widths=(434, 868),
+               processes: int = 0) -> list[tuple[int, int, int]]:
+    """(N, bits, q) per product: N log-uniform over 2^log_n[0]..2^log_n[1], width uniform over
+    `widths`, a seeded prime q of that width per product. With processes > 1 the primes are
+    found by a spawn-context process pool (create it before the process initialises CUDA)."""
+    rng = random.Random(seed)
+    shape = []
+    for i in range(count):
+        N = 1 << rng.randint(*log_n)
+        shape.append((N, rng.choice(list(widths))))
+    jobs = [(bits, seed * 100003 + i) for i, (_, bits) in enumerate(shape)]
+    if processes > 1:
+        import multiprocessing as mp
+
+        with mp.get_context("spawn").Pool(processes) as pool:
+            qs = pool.map(_prime_job, jobs, chunksize=4)
+    else:
+        qs = [gen_prime_fast(*j) for j in jobs]
+    return [(N, bits, q) for (N, bits), q in zip(shape, qs)]
+
+
 def limbs_of(x: int, L: int) -> np.ndarray:
     return np.array([(x >> (32 * i)) & 0xFFFFFFFF for i in range(L)], dtype=np.uint32)
 

@@ -3,9 +3,13 @@
 #include "fherma.h"
 #include "negacyclic_b200.h"
 
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "batch.h"
 #include "engine.h"
@@ -131,29 +135,79 @@ int nc_primes(uint64_t* out, int count) {
 
 // ------------------------------------------------------------------ reference contract
 
+namespace {
+
+// The state behind the contract's void*: the plan, plus the next call's output vector. A
+// std::vector<uint32_t> of N*L elements must be value-initialised before it has that size, a
+// 7 MB memset at N = 65536; a helper thread prepares the next one after each call returns, so
+// fherma_run only moves a ready vector into its Outputs.
+struct FhermaState {
+    nc::Plan* plan = nullptr;
+    std::vector<uint32_t> spare;
+    std::mutex mu;
+    std::condition_variable cv;
+    bool want = false, stop = false;
+    std::thread helper;
+
+    explicit FhermaState(nc::Plan* p) : plan(p), spare(p->limbs()) {
+        helper = std::thread([this] {
+            std::unique_lock<std::mutex> lock(mu);
+            for (;;) {
+                cv.wait(lock, [&] { return want || stop; });
+                if (stop) return;
+                lock.unlock();
+                std::vector<uint32_t> v(plan->limbs());
+                lock.lock();
+                spare = std::move(v);
+                want = false;
+                cv.notify_all();
+            }
+        });
+    }
+    ~FhermaState() {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            stop = true;
+        }
+        cv.notify_all();
+        helper.join();
+        nc::plan_destroy(plan);
+    }
+    std::vector<uint32_t> take() {
+        std::unique_lock<std::mutex> lock(mu);
+        cv.wait(lock, [&] { return !want; });
+        std::vector<uint32_t> v = std::move(spare);
+        want = true;  // the helper builds the next one while the caller uses this one
+        cv.notify_all();
+        return v;
+    }
+};
+
+}  // namespace
+
 void* fherma_init(const fherma::Point& point) {
     if (point.q.data.size() != point.L) throw std::runtime_error("q must hold L limbs");
     try {
         nc::Plan* p = nc::plan_create(point.N, point.W, point.L, point.q.data.data());
-        // init is not timed by the harness: pick the row tiling for this N on the device now
-        const char* tune = std::getenv("NC_AUTOTUNE");
-        if (!(tune && tune[0] == '0')) {
-            try {
-                nc::plan_autotune(p, 3);
-            } catch (...) {
-                nc::plan_destroy(p);
-                throw;
-            }
+        try {
+            // init is not timed by the harness: pick the row tiling for this N on the device now
+            const char* tune = std::getenv("NC_AUTOTUNE");
+            if (!(tune && tune[0] == '0')) nc::plan_autotune(p, 3);
+            nc::ensure_host_path(p);
+            return new FhermaState(p);
+        } catch (...) {
+            nc::plan_destroy(p);
+            throw;
         }
-        return p;
     } catch (const nc::Error& e) {
         throw std::runtime_error(e.what());
     }
 }
 
 fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
-    auto* p = static_cast<nc::Plan*>(state);
-    if (!p) throw std::runtime_error("null state");
+    auto* st = static_cast<FhermaState*>(state);
+    if (!st) throw std::runtime_error("null state");
+    nc::Plan* p = st->plan;
     const size_t count = p->limbs();
     if (in.a.data.size() != count || in.b.data.size() != count)
         throw std::runtime_error("a and b must contain N*L limbs");
@@ -161,7 +215,8 @@ fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
     out.c.shape = {int64_t(p->N), int64_t(p->L)};
     try {
         nc::plan_submit_host(p, in.a.data.data(), in.b.data.data());
-        out.c.data.resize(count);  // zero-fills on the host while the GPU computes
+        out.c.data = st->take();
+        if (out.c.data.size() != count) out.c.data.resize(count);
         nc::plan_collect_host(p, out.c.data.data());
     } catch (const nc::Error& e) {
         throw std::runtime_error(e.what());
@@ -169,7 +224,7 @@ fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
     return out;
 }
 
-void fherma_free(void* state) { nc::plan_destroy(static_cast<nc::Plan*>(state)); }
+void fherma_free(void* state) { delete static_cast<FhermaState*>(state); }
 
 // ------------------------------------------------------------------ tuning and batches
 
@@ -360,15 +415,16 @@ int nc_server_wait(nc_server* server, uint64_t request_id, uint32_t* c, double* 
 }
 
 int nc_server_stats(nc_server* server, double* p50_ms, double* p99_ms, uint64_t* completed, double* products_per_s,
-                    uint64_t* hbm_in_use, uint64_t* batches) {
+                    uint64_t* hbm_in_use, uint64_t* batches, uint64_t* timeouts) {
     return guarded([&] {
         if (!server) throw nc::Error(nc::kEInval, "null server");
         size_t in_use = 0;
-        uint64_t done = 0, b = 0;
-        server->s->stats(p50_ms, p99_ms, &done, products_per_s, &in_use, &b);
+        uint64_t done = 0, b = 0, t = 0;
+        server->s->stats(p50_ms, p99_ms, &done, products_per_s, &in_use, &b, &t);
         if (completed) *completed = done;
         if (hbm_in_use) *hbm_in_use = in_use;
         if (batches) *batches = b;
+        if (timeouts) *timeouts = t;
     });
 }
 

@@ -28,17 +28,23 @@ void ensure(T** p, size_t* cap, size_t count, const char* what) {
 
 Batch::Batch(int device) : device_(device) {
     tables_ = acquire_tables(device);
-    const cudaError_t e = cudaEventCreateWithFlags(&done_, cudaEventDisableTiming);
+    cudaError_t e = cudaEventCreateWithFlags(&done_, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost(&err_host_, 4 * sizeof(uint32_t));
     if (e != cudaSuccess) {
+        if (done_) cudaEventDestroy(done_);
         release_tables(tables_);
         check(e, "batch event");
     }
+    *err_host_ = 0;
 }
+
+bool Batch::failed() const { return ran_ && *err_host_ != 0; }
 
 Batch::~Batch() {
     // wait on the batch's own event (never on the caller's stream, which may be gone)
     if (ran_) cudaEventSynchronize(done_);
     cudaEventDestroy(done_);
+    cudaFreeHost(err_host_);
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
     cudaFree(d_products_);
@@ -136,7 +142,7 @@ void Batch::finalize() {
 
     ensure(reinterpret_cast<char**>(&d_products_), &products_cap_, n * sizeof(BatchProduct), "batch products");
     ensure(&d_items_, &items_cap_, items.size(), "batch items");
-    ensure(&d_state_, &state_cap_, 2 * n + 2, "batch counters");
+    ensure(&d_state_, &state_cap_, 2 * n + 5, "batch counters");
     if (n) check(cudaMemcpy(d_products_, prods.data(), n * sizeof(BatchProduct), cudaMemcpyHostToDevice), "upload");
     if (!items.empty())
         check(cudaMemcpy(d_items_, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice), "upload");
@@ -168,10 +174,11 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
     args.head = d_state_ + 2 * n;
     args.error = d_state_ + 2 * n + 1;
     args.tables = tables_->view();
-    const size_t state_bytes = (2 * n + 2) * sizeof(uint32_t);
+    const size_t state_bytes = (2 * n + 5) * sizeof(uint32_t);
     if (!use_graph) {
         check(cudaMemsetAsync(d_state_, 0, state_bytes, stream), "batch reset");
         check(launch_persistent(args, ctas_, smem_, stream), "persistent launch");
+        check(cudaMemcpyAsync(err_host_, args.error, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), "batch status");
         check(cudaEventRecord(done_, stream), "batch event");
         ran_ = true;
         return;
@@ -190,6 +197,7 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
         check(cudaGraphInstantiate(&exec_, graph_, 0), "graph instantiate");
     }
     check(cudaGraphLaunch(exec_, stream), "graph launch");
+    check(cudaMemcpyAsync(err_host_, args.error, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), "batch status");
     check(cudaEventRecord(done_, stream), "batch event");
     ran_ = true;
 }
@@ -198,9 +206,10 @@ void Batch::synchronize() {
     if (!ran_) return;
     check(cudaEventSynchronize(done_), "batch");
     if (entries_.empty()) return;
-    uint32_t err = 0;
-    check(cudaMemcpy(&err, d_state_ + 2 * entries_.size() + 1, sizeof(err), cudaMemcpyDeviceToHost), "batch status");
-    if (err) throw Error(kETimeout, "a persistent-kernel dependency wait gave up");
+    if (failed())
+        throw Error(kETimeout, "a persistent-kernel dependency wait gave up (stage " + std::to_string(err_host_[1] >> 28) +
+                                   ", product " + std::to_string(err_host_[1] & 0x0fffffffu) + ", saw " +
+                                   std::to_string(err_host_[2]) + " of " + std::to_string(err_host_[3]) + ")");
 }
 
 }  // namespace nc

@@ -35,6 +35,8 @@ class Batch {
     int ctas() const { return ctas_; }
     size_t scratch_bytes() const { return scratch_bytes_; }
     int launches_per_run() const { return 1; }
+    // After the last run has completed (its event): did a dependency wait give up?
+    bool failed() const;
 
   private:
     struct Entry {
@@ -68,6 +70,7 @@ class Batch {
     cudaEvent_t done_ = nullptr;  // recorded after every run
     bool ran_ = false;
     bool dirty_ = true;
+    uint32_t* err_host_ = nullptr;  // pinned copy of the run's error flag, written before done_
 };
 
 }  // namespace nc

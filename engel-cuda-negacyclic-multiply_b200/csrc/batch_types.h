@@ -26,7 +26,7 @@ struct BatchArgs {
     int n_items;
     uint32_t* counters;  // per product: residue items done, row items done
     uint32_t* head;      // next queue position
-    uint32_t* error;     // nonzero once a wait gave up
+    uint32_t* error;     // [0] nonzero once a wait gave up; [1..3] what it waited for
     Tables tables;
 };
 

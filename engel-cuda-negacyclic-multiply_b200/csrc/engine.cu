@@ -115,6 +115,7 @@ void HostPool::run(const std::function<void(int, int)>& fn) {
         fn(0, 1);
         return;
     }
+    std::lock_guard<std::mutex> one_job(run_mu_);  // callers on several threads take turns
     job_ = &fn;
     pending_.store(int(workers_.size()), std::memory_order_relaxed);
     {
@@ -181,30 +182,49 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
     try {
         p->device = current_device();
         p->tables = acquire_tables(p->device);
-        const size_t res = size_t(p->k) * N * sizeof(uint64_t);
-        const size_t limbs = size_t(N) * L * sizeof(uint32_t);
         check(cudaMalloc(&p->d_qc, sizeof(QConst)), "plan constants");
         check(cudaMemcpy(p->d_qc, &p->hq, sizeof(QConst), cudaMemcpyHostToDevice), "plan constants upload");
-        check(cudaMalloc(&p->d_ra, res), "residues a");
-        check(cudaMalloc(&p->d_rb, res), "residues b");
-        check(cudaMalloc(&p->d_a, limbs), "input a");
-        check(cudaMalloc(&p->d_b, limbs), "input b");
-        check(cudaMalloc(&p->d_c, limbs), "output c");
-        check(cudaMallocHost(&p->h_a, limbs), "pinned a");
-        check(cudaMallocHost(&p->h_b, limbs), "pinned b");
-        check(cudaMallocHost(&p->h_c, limbs), "pinned c");
         check(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "stream");
         check(cudaEventCreate(&p->ev_start), "event");
         check(cudaEventCreate(&p->ev_stop), "event");
         for (auto& ev : p->ev_stage) check(cudaEventCreate(&ev), "event");
-        p->pool = new HostPool(copy_threads());
-        p->ev_out.assign(size_t(p->pool->parts()), nullptr);
-        for (auto& ev : p->ev_out) check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
     } catch (...) {
         plan_destroy(p);
         throw;
     }
     return p;
+}
+
+// The plain path's residue scratch (2 k N u64), allocated on its first use: plans used only
+// inside batches or through the allocation-free entry point never hold it.
+void ensure_scratch(Plan* p) {
+    if (p->d_ra) return;
+    const size_t res = size_t(p->k) * p->N * sizeof(uint64_t);
+    check(cudaMalloc(&p->d_ra, res), "residues a");
+    const cudaError_t e = cudaMalloc(&p->d_rb, res);
+    if (e != cudaSuccess) {
+        cudaFree(p->d_ra);
+        p->d_ra = nullptr;
+        check(e, "residues b");
+    }
+}
+
+// Staging for host operands (device copies, pinned buffers, copy threads), on first use.
+void ensure_host_path(Plan* p) {
+    ensure_scratch(p);
+    if (p->pool) return;
+    const size_t limbs = p->limbs() * sizeof(uint32_t);
+    check(cudaMalloc(&p->d_a, limbs), "input a");
+    check(cudaMalloc(&p->d_b, limbs), "input b");
+    check(cudaMalloc(&p->d_c, limbs), "output c");
+    check(cudaMallocHost(&p->h_a, limbs), "pinned a");
+    check(cudaMallocHost(&p->h_b, limbs), "pinned b");
+    check(cudaMallocHost(&p->h_c, limbs), "pinned c");
+    // one set of copy threads per process, shared by every plan (jobs run one at a time)
+    static HostPool* shared = new HostPool(copy_threads());
+    p->ev_out.assign(size_t(shared->parts()), nullptr);
+    for (auto& ev : p->ev_out) check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+    p->pool = shared;
 }
 
 void plan_destroy(Plan* p) {
@@ -226,7 +246,6 @@ void plan_destroy(Plan* p) {
     if (p->stream) cudaStreamDestroy(p->stream);
     for (auto ev : p->ev_out)
         if (ev) cudaEventDestroy(ev);
-    delete p->pool;
     release_tables(p->tables);
     delete p;
 }
@@ -237,6 +256,7 @@ void plan_multiply_device(Plan* p, const uint32_t* d_a, const uint32_t* d_b, uin
     if (((reinterpret_cast<uintptr_t>(d_a) | reinterpret_cast<uintptr_t>(d_b) | reinterpret_cast<uintptr_t>(d_c)) &
          15) != 0)
         throw Error(kEInval, "device buffers must be 16-byte aligned");
+    ensure_scratch(p);
     const ProductDesc d = p->desc(d_a, d_b, d_c);
     check(launch_product(d, p->tables->view(), p->cfg, stream, p->timing ? p->ev_stage : nullptr),
           "kernel launch");
@@ -259,6 +279,7 @@ constexpr size_t kSubChunk = size_t(256) << 10;  // staging granule: memcpy, the
 void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
     if (!p) throw Error(kEInval, "null plan");
     if (!a || !b) throw Error(kEInval, "null host buffer");
+    ensure_host_path(p);
     const size_t bytes = p->limbs() * sizeof(uint32_t);
     std::atomic<int> err{int(cudaSuccess)};
     p->pool->run([&](int part, int parts) {
@@ -297,6 +318,7 @@ void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
 void plan_collect_host(Plan* p, uint32_t* c) {
     if (!p) throw Error(kEInval, "null plan");
     if (!c) throw Error(kEInval, "null host buffer");
+    if (!p->pool) throw Error(kEInval, "collect without a submitted product");
     const size_t bytes = p->limbs() * sizeof(uint32_t);
     std::atomic<int> err{int(cudaSuccess)};
     p->pool->run([&](int part, int parts) {
@@ -345,6 +367,7 @@ void plan_set_row_config(Plan* p, const RowConfig& c) {
 float plan_autotune(Plan* p, int reps) {
     if (!p) throw Error(kEInval, "null plan");
     if (reps < 1) reps = 1;
+    ensure_host_path(p);
     // Operands: the plan's own staging buffers with reduced random limbs (values need not be < q
     // for timing; every limb pattern runs the same instructions).
     const size_t words = p->limbs();

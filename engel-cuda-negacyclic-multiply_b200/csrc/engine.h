@@ -14,7 +14,6 @@
 #include <vector>
 
 #include "common.h"
-#include "stages.cuh"
 
 namespace nc {
 
@@ -55,6 +54,7 @@ class HostPool {
   private:
     void worker(int part);
     std::vector<std::thread> workers_;
+    std::mutex run_mu_;
     std::mutex mu_;
     std::condition_variable cv_;
     std::atomic<uint64_t> gen_{0};
@@ -95,7 +95,11 @@ struct Plan {
 Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q);
 void plan_destroy(Plan* p);
 
-// Device-resident product on `stream` (plan stream when null). Asynchronous.
+// Plain-path resources, allocated on first use (cheap plans for batches and servers).
+void ensure_scratch(Plan* p);
+void ensure_host_path(Plan* p);
+
+// Device-resident product on `stream` (0: the CUDA default stream). Asynchronous.
 void plan_multiply_device(Plan* p, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t stream);
 
 // Host buffers in and out (the fherma_run contract), in two halves so a caller can do host work

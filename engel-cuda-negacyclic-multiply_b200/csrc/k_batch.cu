@@ -22,13 +22,21 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
 }
 
 // Thread 0 only. True once *ctr >= need; false after kSpinLimit polls or once an error is set.
-__device__ bool wait_count(const uint32_t* ctr, uint32_t need, uint32_t* error) {
+// The first wait to give up records what it waited for: error[1] = stage << 28 | product,
+// error[2] = the count it last saw, error[3] = the count it needed.
+__device__ bool wait_count(const uint32_t* ctr, uint32_t need, uint32_t* error, uint32_t what) {
+    uint32_t seen = 0;
     for (uint32_t it = 0; it < kSpinLimit; ++it) {
-        if (ld_acquire(ctr) >= need) return true;
+        seen = ld_acquire(ctr);
+        if (seen >= need) return true;
         if (ld_acquire(error) != 0) return false;
         __nanosleep(it < 64 ? 64 : 512);
     }
-    atomicExch(error, 1u);
+    if (atomicCAS(error, 0u, 1u) == 0u) {
+        error[1] = what;
+        error[2] = seen;
+        error[3] = need;
+    }
     return false;
 }
 
@@ -83,8 +91,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
         const BatchProduct bp = a.products[prod];
         if (threadIdx.x == 0) {
             bool ok = true;
-            if (stage == kItemRow) ok = wait_count(a.counters + 2 * prod, bp.n_dec, a.error);
-            if (stage == kItemCrt) ok = wait_count(a.counters + 2 * prod + 1, bp.n_row, a.error);
+            if (stage == kItemRow) ok = wait_count(a.counters + 2 * prod, bp.n_dec, a.error, w.x);
+            if (stage == kItemCrt) ok = wait_count(a.counters + 2 * prod + 1, bp.n_row, a.error, w.x);
             s_go = ok ? 1 : 0;
         }
         __syncthreads();

@@ -225,11 +225,13 @@ double Server::wait(uint64_t id, uint32_t* c) {
     Request* r = it->second.get();
     done_cv_.wait(lock, [&] { return r->status == 2 || r->status < 0; });
     if (r->status < 0) {
-        const bool memory = r->status == -3;
+        const int r_status = r->status;
+        const bool memory = r_status == -3;
         host_arena_.free(r->host);
         requests_.erase(it);
         space_cv_.notify_all();
         if (memory) throw Error(kENoMem, "the HBM budget cannot hold this request beside the registered operands");
+        if (r_status == -4) throw Error(kETimeout, "the request's batch gave up a dependency wait");
         throw Error(kECuda, "request failed: " + fault_);
     }
     const double latency = r->t_done - r->t_submit;
@@ -245,7 +247,7 @@ double Server::wait(uint64_t id, uint32_t* c) {
 }
 
 void Server::stats(double* p50_ms, double* p99_ms, uint64_t* completed, double* products_per_s, size_t* hbm_in_use,
-                   uint64_t* batches) {
+                   uint64_t* batches, uint64_t* timeouts) {
     std::lock_guard<std::mutex> lock(mu_);
     std::vector<double> v = latencies_;
     auto pct = [&](double f) {
@@ -262,6 +264,7 @@ void Server::stats(double* p50_ms, double* p99_ms, uint64_t* completed, double* 
                                                                         : 1e3 * double(latencies_.size()) / (t_last_ - t_first_);
     if (hbm_in_use) *hbm_in_use = dev_arena_.in_use();
     if (batches) *batches = batches_run_;
+    if (timeouts) *timeouts = timeouts_;
 }
 
 // Scheduler thread: reap finished batches, admit queued requests in order while the HBM budget
@@ -319,10 +322,14 @@ bool Server::reap(bool) {
             continue;
         }
         const double t = now_ms();
+        const bool timed_out = q == cudaSuccess && batches_[size_t(it->stream)]->failed();
+        if (timed_out) ++timeouts_;
         for (Request* r : it->reqs) {
             dev_arena_.free(r->dev);
             r->dev = nullptr;
-            if (q == cudaSuccess) {
+            if (timed_out) {
+                r->status = -4;
+            } else if (q == cudaSuccess) {
                 r->status = 2;
                 r->t_done = t;
                 latencies_.push_back(t - r->t_submit);

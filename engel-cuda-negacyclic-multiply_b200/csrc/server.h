@@ -53,7 +53,7 @@ class Server {
     bool done(uint64_t id);
     double wait(uint64_t id, uint32_t* c);  // milliseconds of latency
     void stats(double* p50_ms, double* p99_ms, uint64_t* completed, double* products_per_s, size_t* hbm_in_use,
-               uint64_t* batches);
+               uint64_t* batches, uint64_t* timeouts = nullptr);
 
   private:
     struct Request {
@@ -104,6 +104,7 @@ class Server {
     std::vector<double> latencies_;
     double t_first_ = -1, t_last_ = 0;
     uint64_t batches_run_ = 0;
+    uint64_t timeouts_ = 0;  // batches whose dependency wait gave up (their requests fail)
     std::thread thread_;
 };
 

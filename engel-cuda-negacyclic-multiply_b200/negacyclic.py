@@ -65,7 +65,7 @@ C_SYMBOLS = [
     ("nc_server_poll", ctypes.c_int, [_vp, ctypes.c_uint64]),
     ("nc_server_wait", ctypes.c_int, [_vp, ctypes.c_uint64, _u32p, ctypes.POINTER(ctypes.c_double)]),
     ("nc_server_stats", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _u64p,
-                                       ctypes.POINTER(ctypes.c_double), _u64p, _u64p]),
+                                       ctypes.POINTER(ctypes.c_double), _u64p, _u64p, _u64p]),
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -307,11 +307,11 @@ class Server:
 
     def stats(self) -> dict:
         p50, p99, pps = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-        done, hbm, batches = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        done, hbm, batches, tmo = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
         _check(load().nc_server_stats(self._h, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(done),
-                                      ctypes.byref(pps), ctypes.byref(hbm), ctypes.byref(batches)))
+                                      ctypes.byref(pps), ctypes.byref(hbm), ctypes.byref(batches), ctypes.byref(tmo)))
         return {"p50_ms": p50.value, "p99_ms": p99.value, "completed": done.value, "products_per_s": pps.value,
-                "hbm_in_use": hbm.value, "batches": batches.value}
+                "hbm_in_use": hbm.value, "batches": batches.value, "timeouts": tmo.value}
 
     def close(self) -> None:
         if self._h:

@@ -1,9 +1,11 @@
 """Run a few device-resident products of one seeded case, for profilers.
 
-    python profile_case.py --N 16384 --bits 868 --reps 3
+    python profile_case.py --N 65536 --bits 868 --reps 3 [--config 12,3,512] [--batch 0]
 
 Each rep enqueues the three kernels of one product (k_dec, k_row, k_crt) on the default
-stream; the run ends by checking the last result against the host entry point.
+stream, with the given row configuration (default: the plan's default); with --batch B > 0
+each rep is instead one persistent launch (k_persistent) of B products. The run ends by
+checking the last result against the host entry point.
 """
 from __future__ import annotations
 
@@ -20,6 +22,8 @@ def main() -> int:
     ap.add_argument("--bits", type=int, default=868)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--config", type=str, default="")
+    ap.add_argument("--batch", type=int, default=0)
     a = ap.parse_args()
 
     import numpy as np
@@ -32,14 +36,26 @@ def main() -> int:
     dev = torch.device("cuda", 0)
     da = torch.from_numpy(case.a.view(np.int32)).to(dev)
     db = torch.from_numpy(case.b.view(np.int32)).to(dev)
-    dc = torch.empty_like(da)
+    count = max(1, a.batch)
+    dcs = [torch.empty_like(da) for _ in range(count)]
     with nc.Plan(case.N, case.q_limbs, W=case.W) as plan:
-        for _ in range(a.reps):
-            plan.multiply_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), 0)
+        if a.config:
+            plan.row_config = tuple(int(x) for x in a.config.split(","))
+        if a.batch > 0:
+            with nc.Batch() as batch:
+                for dc in dcs:
+                    batch.add(plan, da.data_ptr(), db.data_ptr(), dc.data_ptr())
+                for _ in range(a.reps):
+                    batch.run(0, False)
+                batch.synchronize()
+        else:
+            for _ in range(a.reps):
+                plan.multiply_device(da.data_ptr(), db.data_ptr(), dcs[0].data_ptr(), 0)
         torch.cuda.synchronize()
         want = plan.multiply(case.a, case.b)
-    ok = np.array_equal(dc.cpu().numpy().view(np.uint32), want)
-    print(f"N={a.N} bits={a.bits} reps={a.reps} consistent={ok}")
+        cfg = plan.row_config
+    ok = all(np.array_equal(dc.cpu().numpy().view(np.uint32), want) for dc in dcs)
+    print(f"N={a.N} bits={a.bits} reps={a.reps} batch={a.batch} config={cfg} consistent={ok}")
     return 0 if ok else 1
 
 

@@ -157,9 +157,10 @@ int nc_server_submit(nc_server* server, nc_plan* plan, const uint32_t* a, int op
 int nc_server_poll(nc_server* server, uint64_t request_id);
 int nc_server_wait(nc_server* server, uint64_t request_id, uint32_t* c, double* latency_ms);
 /* Latency percentiles over completed requests, their count, completed products per second
-   since the first submit, device bytes in use, batches launched. Pointers may be NULL. */
+   since the first submit, device bytes in use, batches launched, batches whose bounded
+   dependency wait gave up (their requests fail with NC_ETIMEOUT). Pointers may be NULL. */
 int nc_server_stats(nc_server* server, double* p50_ms, double* p99_ms, uint64_t* completed, double* products_per_s,
-                    uint64_t* hbm_in_use, uint64_t* batches);
+                    uint64_t* hbm_in_use, uint64_t* batches, uint64_t* timeouts);
 
 #ifdef __cplusplus
 }

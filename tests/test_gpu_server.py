@@ -115,3 +115,38 @@ def test_oversized_request_is_rejected(gpu, mix):
         with pytest.raises(nc.NegacyclicError) as ei:
             srv.submit(p, reused[0], reused[1])
         assert ei.value.code == nc.NC_ENOMEM
+
+
+def test_high_rate_overlapping_batches(gpu, mix):
+    """Eight clients at a high rate, three streams: batches overlap on the device; every result
+    exact and no batch gives up a dependency wait."""
+    plans, _ = mix
+    want = {}
+    for pi, (p, q, L, reused) in enumerate(plans):
+        want[pi] = p.multiply(reused[0], reused[1])
+    with nc.Server(hbm_budget=4 << 30, staging=1 << 29, max_batch=32, streams=3) as srv:
+        ops = {pi: srv.register_operand(p, reused[0]) for pi, (p, q, L, reused) in enumerate(plans)}
+        errors = []
+
+        def client(c):
+            r = random.Random(c)
+            rids = []
+            for i in range(40):
+                pi = r.randrange(len(plans))
+                p, q, L, reused = plans[pi]
+                cached = r.random() < 0.3
+                rids.append((pi, srv.submit(p, None if cached else reused[0], reused[1], operand=ops[pi] if cached else -1)))
+            for pi, rid in rids:
+                c_, _ = srv.wait(rid, plans[pi][0])
+                if not np.array_equal(c_, want[pi]):
+                    errors.append((c, pi))
+
+        threads = [threading.Thread(target=client, args=(c,)) for c in range(8)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        st = srv.stats()
+    assert st["timeouts"] == 0
+    assert not errors, errors[:5]
+    assert st["completed"] == 320
