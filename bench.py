@@ -385,14 +385,16 @@ def ours(args) -> dict | None:
                          "ms_p50": 1e3 * statistics.median(secs), "init_s": init_s,
                          "via": "fherma_run in the library's harness runner (pageable std::vector in/out)"}
     if forms:
-        log("batched N=65536")
-        result["batched_n65536"] = batched_same_shape(dev, case.q, 65536, 16, args)
-        log("batched 64 x N=16384")
-        result["batched_c3"] = batched_same_shape(dev, case.q, 16384, 64, args)
-        log("uneven batch")
-        result["uneven_c4"] = uneven_batch(dev, mix, args)
-        log("serving")
-        result["serve_c5"] = serving(dev, mix, args)
+        # each form checks its own results; a failure is reported in its entry, not hidden
+        for key, what, fn in (("batched_n65536", "batched N=65536", lambda: batched_same_shape(dev, case.q, 65536, 16, args)),
+                              ("batched_c3", "batched 64 x N=16384", lambda: batched_same_shape(dev, case.q, 16384, 64, args)),
+                              ("uneven_c4", "uneven batch", lambda: uneven_batch(dev, mix, args)),
+                              ("serve_c5", "serving", lambda: serving(dev, mix, args))):
+            log(what)
+            try:
+                result[key] = fn()
+            except Exception as e:
+                result[key] = {"error": f"{type(e).__name__}: {e}"[:500]}
         log("forms done")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(case)
@@ -535,6 +537,9 @@ def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
             enumerate(plans)]
     out = {"budget_bytes": 40 << 30, "requests_per_rate": requests, "reuse_fraction": 0.3, "rates": []}
     try:
+        # every request of plan i multiplies host[i]: one expected product per plan (this also
+        # allocates each plan's staging before any timing)
+        want = [p.multiply(a, b) for (p, _, _), (a, b) in zip(plans, host)]
         for rate in rates:
             sched = []
             t = 0.0
@@ -557,9 +562,18 @@ def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
                         pending.put((pi, srv.submit(p, None if reuse else a, b, operand=opids[pi] if reuse else -1)))
                     pending.put(None)
 
-                def consumer(pending):  # each client collects its results as they come
+                wrong, failed, lat_srv = [], [], []
+
+                def consumer(pending):  # each client collects and checks its results as they come
                     while (item := pending.get()) is not None:
-                        srv.wait(item[1], plans[item[0]][0])
+                        try:
+                            c, ms = srv.wait(item[1], plans[item[0]][0])
+                        except nc.NegacyclicError as e:  # keep draining so staging is released
+                            failed.append(str(e))
+                            continue
+                        lat_srv.append(ms)
+                        if not np.array_equal(c, want[item[0]]):
+                            wrong.append(item[0])
 
                 threads = []
                 for c in range(clients):
@@ -570,12 +584,13 @@ def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
                 for th in threads:
                     th.join()
                 st = srv.stats()
-            row["server"] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "products_per_s": st["products_per_s"],
-                             "batches": st["batches"]}
+            if wrong or failed:
+                raise RuntimeError(f"served products differ from the plain path for plans {sorted(set(wrong))[:8]}; "
+                                   f"{len(failed)} requests failed: {failed[:2]}")
+            row["server"] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": max(lat_srv),
+                             "products_per_s": st["products_per_s"], "batches": st["batches"],
+                             "timeouts": st["timeouts"], "verified": len(lat_srv)}
             # plain per-call form on the same schedule: one worker, host operands in and out
-            if rate == rates[0]:
-                for (p, _, _), (a, b) in zip(plans, host):
-                    p.multiply(a, b)  # first use allocates each plan's staging: keep it out of the timing
             lat = []
             t0 = time.perf_counter()
             for ta, pi, _ in sched:

@@ -50,6 +50,7 @@ Batch::~Batch() {
     cudaFree(d_products_);
     cudaFree(d_items_);
     cudaFree(d_state_);
+    cudaFreeHost(h_upload_);
     cudaFree(scratch_);
     release_tables(tables_);
 }
@@ -78,7 +79,7 @@ void Batch::clear() {
     dirty_ = true;
 }
 
-void Batch::finalize() {
+void Batch::finalize(cudaStream_t stream) {
     // the previous run may still read the device-side product and item tables
     if (ran_) check(cudaEventSynchronize(done_), "batch");
     const size_t n = entries_.size();
@@ -143,9 +144,29 @@ void Batch::finalize() {
     ensure(reinterpret_cast<char**>(&d_products_), &products_cap_, n * sizeof(BatchProduct), "batch products");
     ensure(&d_items_, &items_cap_, items.size(), "batch items");
     ensure(&d_state_, &state_cap_, 2 * n + 5, "batch counters");
-    if (n) check(cudaMemcpy(d_products_, prods.data(), n * sizeof(BatchProduct), cudaMemcpyHostToDevice), "upload");
-    if (!items.empty())
-        check(cudaMemcpy(d_items_, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice), "upload");
+    // Stream-ordered upload from pinned memory: the kernel on `stream` sees the tables only after
+    // the copies (a synchronous copy from pageable memory may return before its DMA lands, and
+    // nothing would order it before a launch on a non-blocking stream). The previous run has
+    // completed (event above), so the pinned buffer is free to rewrite.
+    const size_t prod_bytes = round_up(n * sizeof(BatchProduct), 256);
+    const size_t item_bytes = items.size() * sizeof(uint2);
+    if (prod_bytes + item_bytes > h_upload_cap_) {
+        cudaFreeHost(h_upload_);
+        h_upload_ = nullptr;
+        h_upload_cap_ = 0;
+        const size_t cap = 2 * (prod_bytes + item_bytes);
+        check(cudaMallocHost(&h_upload_, cap), "batch upload staging");
+        h_upload_cap_ = cap;
+    }
+    if (n) {
+        std::memcpy(h_upload_, prods.data(), n * sizeof(BatchProduct));
+        check(cudaMemcpyAsync(d_products_, h_upload_, n * sizeof(BatchProduct), cudaMemcpyHostToDevice, stream),
+              "upload");
+    }
+    if (item_bytes) {
+        std::memcpy(h_upload_ + prod_bytes, items.data(), item_bytes);
+        check(cudaMemcpyAsync(d_items_, h_upload_ + prod_bytes, item_bytes, cudaMemcpyHostToDevice, stream), "upload");
+    }
 
     smem_ = smax(smax(dec_smem_bytes(kmax), crt_smem_bytes(kmax)), row_smem_bytes(kThreads, 4));
     int per_sm = 0, sms = 0;
@@ -164,7 +185,7 @@ void Batch::finalize() {
 
 void Batch::run(cudaStream_t stream, bool use_graph) {
     if (entries_.empty()) return;
-    if (dirty_) finalize();
+    if (dirty_) finalize(stream);
     const size_t n = entries_.size();
     BatchArgs args{};
     args.products = static_cast<const BatchProduct*>(d_products_);
@@ -206,10 +227,14 @@ void Batch::synchronize() {
     if (!ran_) return;
     check(cudaEventSynchronize(done_), "batch");
     if (entries_.empty()) return;
-    if (failed())
-        throw Error(kETimeout, "a persistent-kernel dependency wait gave up (stage " + std::to_string(err_host_[1] >> 28) +
-                                   ", product " + std::to_string(err_host_[1] & 0x0fffffffu) + ", saw " +
-                                   std::to_string(err_host_[2]) + " of " + std::to_string(err_host_[3]) + ")");
+    if (failed()) throw Error(kETimeout, failure());
+}
+
+std::string Batch::failure() const {
+    if (!failed()) return std::string();
+    return "a persistent-kernel dependency wait gave up (stage " + std::to_string(err_host_[1] >> 28) + ", product " +
+           std::to_string(err_host_[1] & 0x0fffffffu) + ", saw " + std::to_string(err_host_[2]) + " of " +
+           std::to_string(err_host_[3]) + ")";
 }
 
 }  // namespace nc

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "engine.h"
@@ -37,6 +38,8 @@ class Batch {
     int launches_per_run() const { return 1; }
     // After the last run has completed (its event): did a dependency wait give up?
     bool failed() const;
+    // What the failed wait waited for (empty when nothing failed).
+    std::string failure() const;
 
   private:
     struct Entry {
@@ -49,7 +52,7 @@ class Batch {
         uint64_t* hat_out;
         uint64_t* scratch;
     };
-    void finalize();
+    void finalize(cudaStream_t stream);
     int device_;
     std::vector<Entry> entries_;
     std::vector<uint64_t> shape_;  // signature of the captured graph
@@ -60,6 +63,8 @@ class Batch {
     size_t items_cap_ = 0;
     uint32_t* d_state_ = nullptr;  // counters (2 per product), head, error
     size_t state_cap_ = 0;
+    char* h_upload_ = nullptr;  // pinned: product table | item list, copied on the run's stream
+    size_t h_upload_cap_ = 0;
     uint64_t* scratch_ = nullptr;
     size_t scratch_bytes_ = 0;
     int n_items_ = 0;

@@ -51,6 +51,9 @@ DeviceTables* acquire_tables(int device) {
         check(cudaMemcpy(t->fwd, h.fwd.data(), tw_bytes, cudaMemcpyHostToDevice), "twiddle upload");
         check(cudaMemcpy(t->inv, h.inv.data(), tw_bytes, cudaMemcpyHostToDevice), "inverse twiddle upload");
         check(prepare_kernels(h.pc.data(), h.pow32.data()), "kernel preparation");
+        // a synchronous copy from pageable memory may return before its last DMA lands, and the
+        // kernels run on non-blocking streams that do not order after it: wait for the device
+        check(cudaDeviceSynchronize(), "table upload");
     } catch (...) {
         cudaFree(t->fwd);
         cudaFree(t->inv);
@@ -183,8 +186,11 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
         p->device = current_device();
         p->tables = acquire_tables(p->device);
         check(cudaMalloc(&p->d_qc, sizeof(QConst)), "plan constants");
-        check(cudaMemcpy(p->d_qc, &p->hq, sizeof(QConst), cudaMemcpyHostToDevice), "plan constants upload");
         check(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "stream");
+        // ordered on the plan's stream and complete before any other stream can use the plan
+        check(cudaMemcpyAsync(p->d_qc, &p->hq, sizeof(QConst), cudaMemcpyHostToDevice, p->stream),
+              "plan constants upload");
+        check(cudaStreamSynchronize(p->stream), "plan constants upload");
         check(cudaEventCreate(&p->ev_start), "event");
         check(cudaEventCreate(&p->ev_stop), "event");
         for (auto& ev : p->ev_stage) check(cudaEventCreate(&ev), "event");
@@ -380,8 +386,9 @@ float plan_autotune(Plan* p, int reps) {
         host[w] = uint32_t(s);
     }
     for (size_t n = 0; n < size_t(p->N); ++n) host[n * p->L + p->L - 1] &= p->hq.q[p->L - 1] >> 1;
-    check(cudaMemcpy(p->d_a, host.data(), words * 4, cudaMemcpyHostToDevice), "tune upload");
-    check(cudaMemcpy(p->d_b, host.data(), words * 4, cudaMemcpyHostToDevice), "tune upload");
+    check(cudaMemcpyAsync(p->d_a, host.data(), words * 4, cudaMemcpyHostToDevice, p->stream), "tune upload");
+    check(cudaMemcpyAsync(p->d_b, host.data(), words * 4, cudaMemcpyHostToDevice, p->stream), "tune upload");
+    check(cudaStreamSynchronize(p->stream), "tune upload");
     const RowConfig saved = p->cfg;
     RowConfig best = saved;
     float best_ms = 1e30f;

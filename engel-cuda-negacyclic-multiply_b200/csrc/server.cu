@@ -231,7 +231,7 @@ double Server::wait(uint64_t id, uint32_t* c) {
         requests_.erase(it);
         space_cv_.notify_all();
         if (memory) throw Error(kENoMem, "the HBM budget cannot hold this request beside the registered operands");
-        if (r_status == -4) throw Error(kETimeout, "the request's batch gave up a dependency wait");
+        if (r_status == -4) throw Error(kETimeout, "the request's batch failed: " + last_timeout_);
         throw Error(kECuda, "request failed: " + fault_);
     }
     const double latency = r->t_done - r->t_submit;
@@ -323,7 +323,10 @@ bool Server::reap(bool) {
         }
         const double t = now_ms();
         const bool timed_out = q == cudaSuccess && batches_[size_t(it->stream)]->failed();
-        if (timed_out) ++timeouts_;
+        if (timed_out) {
+            ++timeouts_;
+            last_timeout_ = batches_[size_t(it->stream)]->failure();
+        }
         for (Request* r : it->reqs) {
             dev_arena_.free(r->dev);
             r->dev = nullptr;

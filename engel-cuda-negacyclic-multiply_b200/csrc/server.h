@@ -105,6 +105,7 @@ class Server {
     double t_first_ = -1, t_last_ = 0;
     uint64_t batches_run_ = 0;
     uint64_t timeouts_ = 0;  // batches whose dependency wait gave up (their requests fail)
+    std::string last_timeout_;  // what the last such wait waited for
     std::thread thread_;
 };
 
