@@ -83,16 +83,20 @@ enum : uint32_t { kModeProduct = 0, kModeCachedA = 1, kModeForward = 2 };
 struct Tables {
     const ulonglong2* fwd;    // [kMaxPrimes][kMaxN]
     const ulonglong2* inv;    // [kMaxPrimes][kMaxN]
+    const uint64_t* pow32;    // [kMaxPrimes][kMaxL]: 2^(32 l) mod p_i
+    const uint64_t* primes;   // [kMaxPrimes]
 };
 
 // Dynamic shared memory of each stage.
 NC_HD constexpr size_t smax(size_t a, size_t b) { return a > b ? a : b; }
-NC_HD constexpr size_t dec_smem_bytes(int k) { return smax(size_t(kTile) * kMaxL * 4, size_t(kTile) * 8 * size_t(k)); }
+// residue stage: limb tile overlaid by the residues, then 2^(32 l) mod p_i and p_i for k primes
+NC_HD constexpr size_t dec_main_bytes(int k) { return smax(size_t(kTile) * kMaxL * 4, size_t(kTile) * 8 * size_t(k)); }
+NC_HD constexpr size_t dec_smem_bytes(int k) { return dec_main_bytes(k) + size_t(k) * (kMaxL + 1) * 8; }
 NC_HD constexpr size_t row_smem_bytes(int threads, int logE) { return size_t(2) * size_t(threads) * (size_t(1) << logE) * 8; }
 NC_HD constexpr size_t crt_smem_bytes(int k) {
     return smax(size_t(kTile) * 8 * size_t(k), size_t(kTile) * kMaxL * 4)  // residues / output staging
            + size_t(k) * kMqStride * 4                                       // M/p_i mod q
-           + size_t(k) * 8 * 2                                               // y, y shoup
+           + size_t(k) * 8 * 3                                               // y, y shoup, p
            + size_t(kMqStride) * 4 * 2 + 16;                                 // -M mod q, q, mu
 }
 

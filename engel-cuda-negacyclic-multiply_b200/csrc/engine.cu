@@ -50,6 +50,15 @@ DeviceTables* acquire_tables(int device) {
         check(cudaMalloc(&t->inv, tw_bytes), "inverse twiddle table");
         check(cudaMemcpy(t->fwd, h.fwd.data(), tw_bytes, cudaMemcpyHostToDevice), "twiddle upload");
         check(cudaMemcpy(t->inv, h.inv.data(), tw_bytes, cudaMemcpyHostToDevice), "inverse twiddle upload");
+        std::vector<uint64_t> primes(kMaxPrimes);
+        for (int i = 0; i < kMaxPrimes; ++i) primes[size_t(i)] = h.pc[size_t(i)].p;
+        check(cudaMalloc(&t->pow32, size_t(kMaxPrimes) * kMaxL * sizeof(uint64_t)), "limb weights");
+        check(cudaMalloc(&t->primes, size_t(kMaxPrimes) * sizeof(uint64_t)), "prime table");
+        check(cudaMemcpy(t->pow32, h.pow32.data(), size_t(kMaxPrimes) * kMaxL * sizeof(uint64_t),
+                         cudaMemcpyHostToDevice),
+              "limb weight upload");
+        check(cudaMemcpy(t->primes, primes.data(), size_t(kMaxPrimes) * sizeof(uint64_t), cudaMemcpyHostToDevice),
+              "prime upload");
         check(prepare_kernels(h.pc.data(), h.pow32.data()), "kernel preparation");
         // a synchronous copy from pageable memory may return before its last DMA lands, and the
         // kernels run on non-blocking streams that do not order after it: wait for the device
@@ -57,6 +66,8 @@ DeviceTables* acquire_tables(int device) {
     } catch (...) {
         cudaFree(t->fwd);
         cudaFree(t->inv);
+        cudaFree(t->pow32);
+        cudaFree(t->primes);
         delete t;
         throw;
     }
@@ -75,6 +86,8 @@ void release_tables(DeviceTables* t) {
     cudaSetDevice(t->device);
     cudaFree(t->fwd);
     cudaFree(t->inv);
+    cudaFree(t->pow32);
+    cudaFree(t->primes);
     cudaSetDevice(prev);
     delete t;
 }
@@ -278,7 +291,18 @@ void slice(size_t bytes, int part, int parts, size_t* lo, size_t* hi) {
     *hi = std::min(bytes, per * size_t(part + 1) * 4096);
 }
 
-constexpr size_t kSubChunk = size_t(256) << 10;  // staging granule: memcpy, then enqueue its DMA
+// Host-to-device copies of a few MB each: on PCIe 5 hosts, copies of a few hundred KB reach well
+// under half the link rate (per-copy overhead), and multi-MB copies reach most of it.
+constexpr size_t kDmaChunk = size_t(4) << 20;
+
+// The product comes back in at most `parts` device-to-host copies of about 2 MB or more (one
+// event each); returns their number and writes their size (a multiple of 4 KiB).
+int out_chunks(size_t bytes, int parts, size_t* chunk) {
+    const size_t want = bytes / (size_t(2) << 20);
+    const int n = int(std::max<size_t>(1, std::min<size_t>(want, size_t(parts))));
+    *chunk = ((bytes + size_t(n) - 1) / size_t(n) + 4095) / 4096 * 4096;
+    return int((bytes + *chunk - 1) / *chunk);
+}
 
 }  // namespace
 
@@ -287,37 +311,38 @@ void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
     if (!a || !b) throw Error(kEInval, "null host buffer");
     ensure_host_path(p);
     const size_t bytes = p->limbs() * sizeof(uint32_t);
-    std::atomic<int> err{int(cudaSuccess)};
-    p->pool->run([&](int part, int parts) {
-        size_t lo, hi;
-        slice(bytes, part, parts, &lo, &hi);
-        const char* srcs[2] = {reinterpret_cast<const char*>(a), reinterpret_cast<const char*>(b)};
-        char* pins[2] = {reinterpret_cast<char*>(p->h_a), reinterpret_cast<char*>(p->h_b)};
-        char* devs[2] = {reinterpret_cast<char*>(p->d_a), reinterpret_cast<char*>(p->d_b)};
-        for (int op = 0; op < 2; ++op)
-            for (size_t off = lo; off < hi; off += kSubChunk) {
-                const size_t n = std::min(kSubChunk, hi - off);
-                std::memcpy(pins[op] + off, srcs[op] + off, n);
-                const cudaError_t e = cudaMemcpyAsync(devs[op] + off, pins[op] + off, n, cudaMemcpyHostToDevice,
-                                                      p->stream);
-                if (e != cudaSuccess) err.store(int(e));
-            }
-    });
-    check(cudaError_t(err.load()), "operand copy");
+    // Each operand goes in equal chunks of at most kDmaChunk: every copy thread stages its part of
+    // a chunk into pinned memory, then the chunk's DMA is enqueued and runs while the next chunk
+    // is staged.
+    const size_t nchunks = (bytes + kDmaChunk - 1) / kDmaChunk;
+    const size_t chunk = ((bytes + nchunks - 1) / nchunks + 4095) / 4096 * 4096;
+    const char* srcs[2] = {reinterpret_cast<const char*>(a), reinterpret_cast<const char*>(b)};
+    char* pins[2] = {reinterpret_cast<char*>(p->h_a), reinterpret_cast<char*>(p->h_b)};
+    char* devs[2] = {reinterpret_cast<char*>(p->d_a), reinterpret_cast<char*>(p->d_b)};
+    for (int op = 0; op < 2; ++op)
+        for (size_t off = 0; off < bytes; off += chunk) {
+            const size_t n = std::min(chunk, bytes - off);
+            p->pool->run([&](int part, int parts) {
+                size_t lo, hi;
+                slice(n, part, parts, &lo, &hi);
+                if (hi > lo) std::memcpy(pins[op] + off + lo, srcs[op] + off + lo, hi - lo);
+            });
+            check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, n, cudaMemcpyHostToDevice, p->stream),
+                  "operand copy");
+        }
     check(cudaEventRecord(p->ev_start, p->stream), "event");
     check(launch_product(p->desc(p->d_a, p->d_b, p->d_c), p->tables->view(), p->cfg, p->stream,
                          p->timing ? p->ev_stage : nullptr),
           "kernel launch");
     check(cudaEventRecord(p->ev_stop, p->stream), "event");
-    const int parts = p->pool->parts();
-    for (int part = 0; part < parts; ++part) {
-        size_t lo, hi;
-        slice(bytes, part, parts, &lo, &hi);
-        if (hi > lo)
-            check(cudaMemcpyAsync(reinterpret_cast<char*>(p->h_c) + lo, reinterpret_cast<char*>(p->d_c) + lo, hi - lo,
-                                  cudaMemcpyDeviceToHost, p->stream),
-                  "product copy");
-        check(cudaEventRecord(p->ev_out[size_t(part)], p->stream), "event");
+    size_t out_chunk;
+    const int nd = out_chunks(bytes, p->pool->parts(), &out_chunk);
+    for (int j = 0; j < nd; ++j) {
+        const size_t lo = size_t(j) * out_chunk, n = std::min(out_chunk, bytes - lo);
+        check(cudaMemcpyAsync(reinterpret_cast<char*>(p->h_c) + lo, reinterpret_cast<char*>(p->d_c) + lo, n,
+                              cudaMemcpyDeviceToHost, p->stream),
+              "product copy");
+        check(cudaEventRecord(p->ev_out[size_t(j)], p->stream), "event");
     }
 }
 
@@ -326,17 +351,21 @@ void plan_collect_host(Plan* p, uint32_t* c) {
     if (!c) throw Error(kEInval, "null host buffer");
     if (!p->pool) throw Error(kEInval, "collect without a submitted product");
     const size_t bytes = p->limbs() * sizeof(uint32_t);
+    size_t out_chunk;
+    out_chunks(bytes, p->pool->parts(), &out_chunk);
     std::atomic<int> err{int(cudaSuccess)};
     p->pool->run([&](int part, int parts) {
-        const cudaError_t e = cudaEventSynchronize(p->ev_out[size_t(part)]);
+        size_t lo, hi;
+        slice(bytes, part, parts, &lo, &hi);
+        if (hi <= lo) return;
+        // the device-to-host chunks complete in order: the one holding this part's last byte
+        // completes after every earlier one
+        const cudaError_t e = cudaEventSynchronize(p->ev_out[(hi - 1) / out_chunk]);
         if (e != cudaSuccess) {
             err.store(int(e));
             return;
         }
-        size_t lo, hi;
-        slice(bytes, part, parts, &lo, &hi);
-        if (hi > lo)
-            std::memcpy(reinterpret_cast<char*>(c) + lo, reinterpret_cast<const char*>(p->h_c) + lo, hi - lo);
+        std::memcpy(reinterpret_cast<char*>(c) + lo, reinterpret_cast<const char*>(p->h_c) + lo, hi - lo);
     });
     check(cudaError_t(err.load()), "product");
     check(cudaStreamSynchronize(p->stream), "product");

@@ -34,7 +34,9 @@ struct DeviceTables {
     int refs = 0;
     ulonglong2* fwd = nullptr;
     ulonglong2* inv = nullptr;
-    Tables view() const { return Tables{fwd, inv}; }
+    uint64_t* pow32 = nullptr;   // [kMaxPrimes][kMaxL]
+    uint64_t* primes = nullptr;  // [kMaxPrimes]
+    Tables view() const { return Tables{fwd, inv, pow32, primes}; }
 };
 
 DeviceTables* acquire_tables(int device);

@@ -59,9 +59,12 @@ __device__ __forceinline__ void load_tile(const uint32_t* x, int N2, int L, int 
 
 // Thread t owns coefficient t of the tile: its limbs stay in registers while it walks the
 // primes two at a time (two independent carry chains), writing residues in [0, 2p) to
-// s_res[i * T + t]. s_res overlays the limb tile, so the limbs are read first.
+// s_res[i * T + t]. s_res overlays the limb tile, so the limbs are read first. The weights
+// 2^(32 l) mod p_i come from shared memory (s_pow, row stride kMaxL): every lane reads the same
+// word, one broadcast per warp, which keeps them off the constant-load path.
 template <int LW>
-__device__ __forceinline__ void dec_residues(const uint32_t* s_in, int L, int k, int T, uint64_t* s_res) {
+__device__ __forceinline__ void dec_residues(const uint32_t* s_in, int L, int k, int T, const uint64_t* s_pow,
+                                             uint64_t* s_res) {
     const int t = threadIdx.x;
     const bool active = t < T;
     uint32_t x[LW];
@@ -98,8 +101,8 @@ __device__ __forceinline__ void dec_residues(const uint32_t* s_in, int L, int k,
 #pragma unroll 1
     for (int i = 0; i < k; i += 2) {
         const int i2 = (i + 1 < k) ? i + 1 : i;
-        const uint64_t* c1 = c_pow32 + i * kMaxL;
-        const uint64_t* c2 = c_pow32 + i2 * kMaxL;
+        const uint64_t* c1 = s_pow + i * kMaxL;
+        const uint64_t* c2 = s_pow + i2 * kMaxL;
         uint32_t a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
         uint32_t e0 = 0, e1 = 0, e2 = 0, f0 = 0, f1 = 0, f2 = 0;
 #pragma unroll
@@ -154,8 +157,10 @@ __device__ __forceinline__ void column_inverse(const ulonglong2* tw, uint64_t p,
 }
 
 // Items (prime i, column j) of the tile: column transform from s_res, store the residue rows.
+// A warp may span two primes, so p_i comes from shared memory (s_p) rather than constant memory.
 template <int LOG_N1>
-__device__ void dec_columns(const Tables& t, int k, int N, int T, int j0, const uint64_t* s_res, uint64_t* R) {
+__device__ void dec_columns(const Tables& t, int k, int N, int T, int j0, const uint64_t* s_res, const uint64_t* s_p,
+                            uint64_t* R) {
     constexpr int N1 = 1 << LOG_N1;
     const int C = T >> LOG_N1;
     const int N2 = N >> LOG_N1;
@@ -164,7 +169,7 @@ __device__ void dec_columns(const Tables& t, int k, int N, int T, int j0, const 
         uint64_t v[N1];
 #pragma unroll
         for (int u = 0; u < N1; ++u) v[u] = s_res[size_t(i) * T + u * C + j];
-        if (LOG_N1 > 0) column_forward<LOG_N1>(t.fwd + size_t(i) * kMaxN, c_pc[i].p, v);
+        if (LOG_N1 > 0) column_forward<LOG_N1>(t.fwd + size_t(i) * kMaxN, s_p[i], v);
         uint64_t* row = R + size_t(i) * N + j0 + j;
 #pragma unroll
         for (int u = 0; u < N1; ++u) __stcg(row + size_t(u) * N2, v[u]);
@@ -182,20 +187,24 @@ __device__ void dec_tile(const ProductDesc& d, const Tables& t, int operand, int
     uint64_t* R = operand ? d.rb : d.ra;
     uint32_t* s_in = reinterpret_cast<uint32_t*>(smem);
     uint64_t* s_res = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* s_pow = reinterpret_cast<uint64_t*>(smem + dec_main_bytes(k));
+    uint64_t* s_p = s_pow + size_t(k) * kMaxL;
     const int j0 = tile * C;
 
     __syncthreads();  // the previous user of shared memory (persistent CTAs) is done
     load_tile(x, N >> logN1, L, j0, C, 1 << logN1, s_in);
+    for (int w = threadIdx.x; w < k * kMaxL; w += blockDim.x) s_pow[w] = __ldg(t.pow32 + w);
+    for (int w = threadIdx.x; w < k; w += blockDim.x) s_p[w] = __ldg(t.primes + w);
     __syncthreads();
-    dec_residues<LW>(s_in, L, k, T, s_res);
+    dec_residues<LW>(s_in, L, k, T, s_pow, s_res);
     __syncthreads();
     switch (logN1) {
-        case 0: dec_columns<0>(t, k, N, T, j0, s_res, R); break;
-        case 1: dec_columns<1>(t, k, N, T, j0, s_res, R); break;
-        case 2: dec_columns<2>(t, k, N, T, j0, s_res, R); break;
-        case 3: dec_columns<3>(t, k, N, T, j0, s_res, R); break;
-        case 4: dec_columns<4>(t, k, N, T, j0, s_res, R); break;
-        default: dec_columns<5>(t, k, N, T, j0, s_res, R); break;
+        case 0: dec_columns<0>(t, k, N, T, j0, s_res, s_p, R); break;
+        case 1: dec_columns<1>(t, k, N, T, j0, s_res, s_p, R); break;
+        case 2: dec_columns<2>(t, k, N, T, j0, s_res, s_p, R); break;
+        case 3: dec_columns<3>(t, k, N, T, j0, s_res, s_p, R); break;
+        case 4: dec_columns<4>(t, k, N, T, j0, s_res, s_p, R); break;
+        default: dec_columns<5>(t, k, N, T, j0, s_res, s_p, R); break;
     }
 }
 
@@ -405,7 +414,7 @@ __device__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint
 // stage 3: inverse column stages + CRT + Barrett
 
 template <int LOG_N1>
-__device__ void crt_columns(const ProductDesc& d, const Tables& t, int tile, uint64_t* s_res) {
+__device__ void crt_columns(const ProductDesc& d, const Tables& t, int tile, const uint64_t* s_p, uint64_t* s_res) {
     constexpr int N1 = 1 << LOG_N1;
     const int N = 1 << d.logN;
     const int N2 = N >> LOG_N1;
@@ -419,7 +428,7 @@ __device__ void crt_columns(const ProductDesc& d, const Tables& t, int tile, uin
         uint64_t v[N1];
 #pragma unroll
         for (int u = 0; u < N1; ++u) v[u] = __ldcg(row + size_t(u) * N2);
-        if (LOG_N1 > 0) column_inverse<LOG_N1>(t.inv + size_t(i) * kMaxN, c_pc[i].p, v);
+        if (LOG_N1 > 0) column_inverse<LOG_N1>(t.inv + size_t(i) * kMaxN, s_p[i], v);
 #pragma unroll
         for (int u = 0; u < N1; ++u) s_res[size_t(i) * T + u * C + j] = v[u];
     }
@@ -537,7 +546,8 @@ __device__ void crt_coeffs(const ProductDesc& d, const Tables& t, int tile, uint
     cur += size_t(k) * kMqStride * 4;
     uint64_t* s_y = reinterpret_cast<uint64_t*>(cur);
     uint64_t* s_ys = s_y + k;
-    cur += size_t(k) * 8 * 2;
+    uint64_t* s_p = s_ys + k;
+    cur += size_t(k) * 8 * 3;
     uint32_t* s_negm = reinterpret_cast<uint32_t*>(cur);
     uint32_t* s_q = s_negm + kMqStride;
     uint32_t* s_mu = s_q + kMqStride;
@@ -548,20 +558,22 @@ __device__ void crt_coeffs(const ProductDesc& d, const Tables& t, int tile, uint
     for (int w = threadIdx.x; w < k; w += blockDim.x) {
         s_y[w] = __ldg(qc->y + w);
         s_ys[w] = __ldg(qc->ys + w);
+        s_p[w] = __ldg(t.primes + w);
     }
     for (int w = threadIdx.x; w < kMqStride; w += blockDim.x) {
         s_negm[w] = __ldg(qc->neg_m + w);
         s_q[w] = __ldg(qc->q + w);
     }
     if (threadIdx.x < 4) s_mu[threadIdx.x] = __ldg(qc->mu + threadIdx.x);
+    __syncthreads();  // s_p is read by the column stages
 
     switch (logN1) {
-        case 0: crt_columns<0>(d, t, tile, s_res); break;
-        case 1: crt_columns<1>(d, t, tile, s_res); break;
-        case 2: crt_columns<2>(d, t, tile, s_res); break;
-        case 3: crt_columns<3>(d, t, tile, s_res); break;
-        case 4: crt_columns<4>(d, t, tile, s_res); break;
-        default: crt_columns<5>(d, t, tile, s_res); break;
+        case 0: crt_columns<0>(d, t, tile, s_p, s_res); break;
+        case 1: crt_columns<1>(d, t, tile, s_p, s_res); break;
+        case 2: crt_columns<2>(d, t, tile, s_p, s_res); break;
+        case 3: crt_columns<3>(d, t, tile, s_p, s_res); break;
+        case 4: crt_columns<4>(d, t, tile, s_p, s_res); break;
+        default: crt_columns<5>(d, t, tile, s_p, s_res); break;
     }
     __syncthreads();
 
