@@ -389,6 +389,7 @@ def ours(args) -> dict | None:
         for key, what, fn in (("batched_n65536", "batched N=65536", lambda: batched_same_shape(dev, case.q, 65536, 16, args)),
                               ("batched_c3", "batched 64 x N=16384", lambda: batched_same_shape(dev, case.q, 16384, 64, args)),
                               ("uneven_c4", "uneven batch", lambda: uneven_batch(dev, mix, args)),
+                              ("ablation_residues", "residue ablation", lambda: residue_ablation(dev, case)),
                               ("serve_c5", "serving", lambda: serving(dev, mix, args))):
             log(what)
             try:
@@ -419,6 +420,57 @@ def _event_ms(fn, warmup: int, reps: int) -> float:
     e1.record()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def residue_ablation(dev, case, reps: int = 20) -> dict:
+    """Residue stage alone for both operands of the main workload, by the integer pipes (the
+    product path's arithmetic) and by the INT8 tensor-core contraction; L2 flushed before each
+    timed pair; both engines' residues compared bit for bit."""
+    import numpy as np
+    import torch
+
+    import negacyclic as nc
+
+    with nc.Plan(case.N, case.q_limbs, W=case.W) as plan:
+        k, N, L = plan.k, plan.N, plan.L
+        da = torch.from_numpy(case.a.view(np.int32)).to(dev)
+        db = torch.from_numpy(case.b.view(np.int32)).to(dev)
+        flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+        outs, ms = {}, {}
+        for name, engine in (("imad", nc.RESIDUES_IMAD), ("tc_i8", nc.RESIDUES_TC_I8)):
+            r = torch.empty(2 * k * N, dtype=torch.int64, device=dev)
+            ra, rb = r.data_ptr(), r.data_ptr() + k * N * 8
+
+            def pair():
+                plan.residues(da.data_ptr(), ra, engine)
+                plan.residues(db.data_ptr(), rb, engine)
+
+            for _ in range(3):
+                pair()
+            times = []
+            for _ in range(reps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                pair()
+                e1.record()
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+            if nc.residues_gave_up():
+                raise RuntimeError("a tensor-core residue launch gave up its wait")
+            outs[name] = r
+            ms[name] = statistics.median(times)
+        exact = bool(torch.equal(outs["imad"], outs["tc_i8"]))
+    if not exact:
+        raise RuntimeError("the two residue engines disagree")
+    hbm_bytes = 2 * (N * L * 4 + k * N * 8)
+    macs = 2 * k * N * L  # u32 x u64 limb MACs of the integer engine
+    return {"what": "residues x mod p_i of both operands (k x N u64 each), N=65536, 868-bit q, k=29",
+            "imad_us": 1e3 * ms["imad"], "tc_i8_us": 1e3 * ms["tc_i8"], "speedup": ms["imad"] / ms["tc_i8"],
+            "bit_exact": exact, "tc_i8_hbm_gbs": hbm_bytes / (ms["tc_i8"] * 1e-3) / 1e9,
+            "tc_i8_int8_tops": 2 * 2 * 128 * (8 * ((k + 1) & ~1)) * N / (ms["tc_i8"] * 1e-3) / 1e12,
+            "imad_limb_macs_per_s": macs / (ms["imad"] * 1e-3), "hbm_bytes": hbm_bytes,
+            "l2": "flushed (256 MiB write) before each timed pair"}
 
 
 def batched_same_shape(dev, q: int, N: int, count: int, args) -> dict:

@@ -49,6 +49,7 @@ cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32) {
     if (e == cudaSuccess) e = prepare_row(pc, pow32);
     if (e == cudaSuccess) e = prepare_crt(pc, pow32);
     if (e == cudaSuccess) e = prepare_persistent(pc, pow32);
+    if (e == cudaSuccess) e = prepare_residues(pc, pow32);
     return e;
 }
 

@@ -41,6 +41,8 @@ C_SYMBOLS = [
     ("nc_plan_stage_ms", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("nc_imad_peak", ctypes.c_int, [ctypes.POINTER(ctypes.c_double)]),
     ("nc_primes", ctypes.c_int, [_u64p, ctypes.c_int]),
+    ("nc_residues", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
+    ("nc_residues_status", ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     ("nc_row_variants", ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
     ("nc_plan_set_row_config", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nc_plan_get_row_config", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
@@ -118,6 +120,17 @@ def primes(count: int = 48) -> list[int]:
     return list(out)
 
 
+RESIDUES_IMAD, RESIDUES_TC_I8 = 0, 1
+
+
+def residues_gave_up() -> bool:
+    """True if a tensor-core residue launch on the current device gave up its bounded wait since the
+    last call (read after the work has finished)."""
+    v = ctypes.c_int()
+    _check(load().nc_residues_status(ctypes.byref(v)))
+    return bool(v.value)
+
+
 class Plan:
     """One (N, q) configuration on the current CUDA device."""
 
@@ -153,6 +166,11 @@ class Plan:
         memory at call time. Its residue scratch is one 8 MiB array inside the library shared by
         all calls (so overlapping calls race); limit k * N <= 2^19 (N <= 16384 at an 868-bit q)."""
         _check(load().nc_multiply_device_noalloc(self._h, _vp(d_a), _vp(d_b), _vp(d_c), _vp(stream or None)))
+
+    def residues(self, d_x: int, d_r: int, engine: int = 0, stream: int = 0) -> None:
+        """Residue stage alone (an ablation): d_r[i * N + n] = x_n mod p_i, k * N u64, by the integer
+        pipes (RESIDUES_IMAD) or an exact INT8 tensor-core contraction (RESIDUES_TC_I8)."""
+        _check(load().nc_residues(self._h, _vp(d_x), _vp(d_r), int(engine), _vp(stream or None)))
 
     def synchronize(self) -> None:
         _check(load().nc_plan_synchronize(self._h))

@@ -91,6 +91,24 @@ int nc_imad_peak(double* ops_per_second);
 /* Residue primes of the fixed set (p = 2^62 - m, p = 1 mod 2^17), first `count` of 48. */
 int nc_primes(uint64_t* out, int count);
 
+/* ------------------------------------------------------------------ residue-stage ablation
+ *
+ * The residue stage alone, r[i * N + n] = x_n mod p_i (canonical, natural coefficient order,
+ * prime-major: k * N u64 in d_r), for the plan's k primes, by one of two engines:
+ *   NC_RESIDUES_IMAD   the product path's own arithmetic: each 32-bit limb times 2^(32 l) mod p_i,
+ *                      accumulated exactly in 32-bit carry chains on the integer pipes;
+ *   NC_RESIDUES_TC_I8  an exact INT8 tensor-core contraction: the bytes of x_n times the bytes of
+ *                      2^(8 j) mod p_i (tcgen05.mma kind::i8, s32 accumulators in tensor memory),
+ *                      recombined and reduced mod p_i; at most 32 primes (q up to about 960 bits).
+ * The counterpart of both in the reference is to_residues_tiled_kernel (solve.cu:533-570), which
+ * also multiplies by R^2 and psi^n. Not used by the product path: it exists to time the two engines
+ * on the same input and check that they agree. d_x is 16-byte aligned; enqueued on `stream`. */
+enum { NC_RESIDUES_IMAD = 0, NC_RESIDUES_TC_I8 = 1 };
+int nc_residues(const nc_plan* plan, const uint32_t* d_x, uint64_t* d_r, int engine, void* stream);
+/* After the work has finished: 1 in *gave_up if a tensor-core launch on the current device gave up
+   its bounded wait for the MMA (its residues are then not written); the flag is cleared. */
+int nc_residues_status(int* gave_up);
+
 /* ------------------------------------------------------------------ tuning */
 
 /* Row-stage tiling of the plan's plain path: row blocks of 2^log_block residues, 2^log_radix
@@ -143,7 +161,10 @@ uint64_t nc_plan_hat_words(const nc_plan* plan);
  * requests into further batches while earlier ones run, so their work overlaps on the device.
  * Operands registered with nc_server_register_operand stay resident in their NTT-domain form;
  * requests that name one (a = NULL, operand_id >= 0) skip its transform. nc_server_wait returns
- * the product and the request's latency from submit to result in pinned host memory. */
+ * the product and the request's latency from submit to result in pinned host memory. A request
+ * holds its staging (3 N L u32) from submit until nc_server_wait collects it, so callers that
+ * submit many requests before collecting any must size staging for all of them, or submit blocks
+ * for good. */
 
 typedef struct nc_server nc_server;
 

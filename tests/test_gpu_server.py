@@ -124,7 +124,9 @@ def test_high_rate_overlapping_batches(gpu, mix):
     want = {}
     for pi, (p, q, L, reused) in enumerate(plans):
         want[pi] = p.multiply(reused[0], reused[1])
-    with nc.Server(hbm_budget=4 << 30, staging=1 << 29, max_batch=32, streams=3) as srv:
+    # every client submits all 40 requests before it waits, and a result holds its pinned staging
+    # until wait(): the 320 requests (~622 MB of staging) must all fit at once
+    with nc.Server(hbm_budget=4 << 30, staging=1 << 31, max_batch=32, streams=3) as srv:
         ops = {pi: srv.register_operand(p, reused[0]) for pi, (p, q, L, reused) in enumerate(plans)}
         errors = []
 
