@@ -243,12 +243,19 @@ void ensure_host_path(Plan* p) {
     static HostPool* shared = new HostPool(copy_threads());
     p->ev_out.assign(size_t(shared->parts()), nullptr);
     for (auto& ev : p->ev_out) check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+    check(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
+    check(cudaEventCreateWithFlags(&p->ev_a, cudaEventDisableTiming), "event");
+    check(cudaEventCreateWithFlags(&p->ev_b, cudaEventDisableTiming), "event");
     p->pool = shared;
 }
 
 void plan_destroy(Plan* p) {
     if (!p) return;
+    if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
     if (p->stream) cudaStreamSynchronize(p->stream);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+    if (p->ev_a) cudaEventDestroy(p->ev_a);
+    if (p->ev_b) cudaEventDestroy(p->ev_b);
     cudaFree(p->d_qc);
     cudaFree(p->d_ra);
     cudaFree(p->d_rb);
@@ -313,13 +320,21 @@ void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
     const size_t bytes = p->limbs() * sizeof(uint32_t);
     // Each operand goes in equal chunks of at most kDmaChunk: every copy thread stages its part of
     // a chunk into pinned memory, then the chunk's DMA is enqueued and runs while the next chunk
-    // is staged.
+    // is staged. Operand a goes on the plan's stream; operand b on the copy stream, after a's
+    // upload (so a arrives first at full link rate), and a's residue stage runs while b uploads.
     const size_t nchunks = (bytes + kDmaChunk - 1) / kDmaChunk;
     const size_t chunk = ((bytes + nchunks - 1) / nchunks + 4095) / 4096 * 4096;
     const char* srcs[2] = {reinterpret_cast<const char*>(a), reinterpret_cast<const char*>(b)};
     char* pins[2] = {reinterpret_cast<char*>(p->h_a), reinterpret_cast<char*>(p->h_b)};
     char* devs[2] = {reinterpret_cast<char*>(p->d_a), reinterpret_cast<char*>(p->d_b)};
-    for (int op = 0; op < 2; ++op)
+    cudaStream_t streams[2] = {p->stream, p->copy_stream};
+    for (int op = 0; op < 2; ++op) {
+        if (op == 1) {
+            // b's buffers may still be read by the plan's stream (a previous product): order the
+            // copy stream after everything enqueued there so far, including a's upload
+            check(cudaEventRecord(p->ev_a, p->stream), "event");
+            check(cudaStreamWaitEvent(p->copy_stream, p->ev_a, 0), "stream wait");
+        }
         for (size_t off = 0; off < bytes; off += chunk) {
             const size_t n = std::min(chunk, bytes - off);
             p->pool->run([&](int part, int parts) {
@@ -327,12 +342,14 @@ void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
                 slice(n, part, parts, &lo, &hi);
                 if (hi > lo) std::memcpy(pins[op] + off + lo, srcs[op] + off + lo, hi - lo);
             });
-            check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, n, cudaMemcpyHostToDevice, p->stream),
+            check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, n, cudaMemcpyHostToDevice, streams[op]),
                   "operand copy");
         }
+    }
+    check(cudaEventRecord(p->ev_b, p->copy_stream), "event");
     check(cudaEventRecord(p->ev_start, p->stream), "event");
     check(launch_product(p->desc(p->d_a, p->d_b, p->d_c), p->tables->view(), p->cfg, p->stream,
-                         p->timing ? p->ev_stage : nullptr),
+                         p->timing ? p->ev_stage : nullptr, p->ev_b),
           "kernel launch");
     check(cudaEventRecord(p->ev_stop, p->stream), "event");
     size_t out_chunk;
@@ -353,19 +370,24 @@ void plan_collect_host(Plan* p, uint32_t* c) {
     const size_t bytes = p->limbs() * sizeof(uint32_t);
     size_t out_chunk;
     out_chunks(bytes, p->pool->parts(), &out_chunk);
+    const int nd = int((bytes + out_chunk - 1) / out_chunk);
     std::atomic<int> err{int(cudaSuccess)};
+    // Every copy thread takes its share of each chunk as soon as that chunk has landed, so the
+    // copy-out after the last transfer is one chunk split over all threads.
     p->pool->run([&](int part, int parts) {
-        size_t lo, hi;
-        slice(bytes, part, parts, &lo, &hi);
-        if (hi <= lo) return;
-        // the device-to-host chunks complete in order: the one holding this part's last byte
-        // completes after every earlier one
-        const cudaError_t e = cudaEventSynchronize(p->ev_out[(hi - 1) / out_chunk]);
-        if (e != cudaSuccess) {
-            err.store(int(e));
-            return;
+        for (int j = 0; j < nd; ++j) {
+            const cudaError_t e = cudaEventSynchronize(p->ev_out[size_t(j)]);
+            if (e != cudaSuccess) {
+                err.store(int(e));
+                return;
+            }
+            const size_t base = size_t(j) * out_chunk, n = std::min(out_chunk, bytes - base);
+            size_t lo, hi;
+            slice(n, part, parts, &lo, &hi);
+            if (hi > lo)
+                std::memcpy(reinterpret_cast<char*>(c) + base + lo, reinterpret_cast<const char*>(p->h_c) + base + lo,
+                            hi - lo);
         }
-        std::memcpy(reinterpret_cast<char*>(c) + lo, reinterpret_cast<const char*>(p->h_c) + lo, hi - lo);
     });
     check(cudaError_t(err.load()), "product");
     check(cudaStreamSynchronize(p->stream), "product");

@@ -82,6 +82,8 @@ struct Plan {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     std::vector<cudaEvent_t> ev_out;  // one per output chunk (one chunk per pool part)
+    cudaStream_t copy_stream = nullptr;         // host path: operand b's upload
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // operand a uploaded / operand b uploaded
     DeviceTables* tables = nullptr;
     HostPool* pool = nullptr;
     float last_kernel_ms = 0.f;

@@ -54,7 +54,7 @@ cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32) {
 }
 
 cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s,
-                           cudaEvent_t* ev) {
+                           cudaEvent_t* ev, cudaEvent_t b_ready) {
     if (int(d.logN2) != cfg.logN2) return cudaErrorInvalidValue;
     void* row = row_kernel(cfg);
     void* dec = dec_kernel(int(d.LW));
@@ -65,7 +65,15 @@ cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfi
     Tables tt = t;
     cudaError_t e;
     if (ev && (e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
-    {
+    if (b_ready && d.mode == kModeProduct) {
+        int tiles = g.tiles;
+        for (int first = 0; first < 2; ++first) {
+            if (first == 1 && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
+            void* args[] = {&dd, &tt, &first, &tiles};
+            e = launch(dec, g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);
+            if (e != cudaSuccess) return e;
+        }
+    } else {
         int first = d.mode == kModeCachedA ? 1 : 0;
         int count = d.mode == kModeProduct ? 2 : 1;
         int tiles = g.tiles;

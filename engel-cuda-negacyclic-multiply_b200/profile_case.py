@@ -4,8 +4,10 @@
 
 Each rep enqueues the three kernels of one product (k_dec, k_row, k_crt) on the default
 stream, with the given row configuration (default: the plan's default); with --batch B > 0
-each rep is instead one persistent launch (k_persistent) of B products. The run ends by
-checking the last result against the host entry point.
+each rep is instead one persistent launch (k_persistent) of B products; with --residues
+imad|tc each rep is the residue stage alone of both operands (k_residues_imad or k_residues_tc).
+The run ends by checking the last result against the host entry point (or, for --residues,
+against the other residue engine).
 """
 from __future__ import annotations
 
@@ -24,10 +26,16 @@ def main() -> int:
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--config", type=str, default="")
     ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--residues", choices=["", "imad", "tc"], default="",
+                    help="run only the residue stage of both operands with this engine (k_residues_imad / "
+                         "k_residues_tc), checked against the other engine")
     a = ap.parse_args()
 
     import numpy as np
     import torch
+
+    if a.residues:
+        return residues_only(a)
 
     import cases
     import negacyclic as nc
@@ -56,6 +64,33 @@ def main() -> int:
         cfg = plan.row_config
     ok = all(np.array_equal(dc.cpu().numpy().view(np.uint32), want) for dc in dcs)
     print(f"N={a.N} bits={a.bits} reps={a.reps} batch={a.batch} config={cfg} consistent={ok}")
+    return 0 if ok else 1
+
+
+def residues_only(a) -> int:
+    import numpy as np
+    import torch
+
+    import cases
+    import negacyclic as nc
+
+    case = cases.make_case(a.N, a.bits, a.seed, edge_frac=0.01)
+    dev = torch.device("cuda", 0)
+    engine = nc.RESIDUES_TC_I8 if a.residues == "tc" else nc.RESIDUES_IMAD
+    other = nc.RESIDUES_IMAD if engine == nc.RESIDUES_TC_I8 else nc.RESIDUES_TC_I8
+    with nc.Plan(case.N, case.q_limbs, W=case.W) as plan:
+        k, N = plan.k, plan.N
+        xs = [torch.from_numpy(x.view(np.int32)).to(dev) for x in (case.a, case.b)]
+        r = torch.empty(2 * k * N, dtype=torch.int64, device=dev)
+        check = torch.empty_like(r)
+        for _ in range(a.reps):
+            for j, x in enumerate(xs):
+                plan.residues(x.data_ptr(), r.data_ptr() + j * k * N * 8, engine)
+        for j, x in enumerate(xs):
+            plan.residues(x.data_ptr(), check.data_ptr() + j * k * N * 8, other)
+        torch.cuda.synchronize()
+        ok = bool(torch.equal(r, check)) and not nc.residues_gave_up()
+    print(f"residues N={a.N} bits={a.bits} reps={a.reps} engine={a.residues} consistent={ok}")
     return 0 if ok else 1
 
 

@@ -74,7 +74,9 @@ int nc_plan_synchronize(nc_plan* plan);
 /* N, L, number of residue primes k, and bit length of q. Any pointer may be NULL. */
 int nc_plan_query(const nc_plan* plan, uint32_t* N, uint32_t* L, uint32_t* k, uint32_t* qbits);
 
-/* Device milliseconds of the kernels of the last nc_multiply (CUDA events). */
+/* Device milliseconds from the first kernel of the last nc_multiply to its last (CUDA events).
+   Operand b uploads while operand a's residue stage runs, so any part of that upload not hidden
+   behind it is included. */
 float nc_plan_last_kernel_ms(const nc_plan* plan);
 
 /* Per-stage device timing of the plan's products: when enabled, each product records CUDA
