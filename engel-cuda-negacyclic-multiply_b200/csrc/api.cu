@@ -81,6 +81,24 @@ int nc_multiply_device(nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, 
     });
 }
 
+int nc_plan_set_crt_engine(nc_plan* plan, int engine) {
+    return guarded([&] {
+        if (!plan) throw nc::Error(nc::kEInval, "null plan");
+        if (engine != NC_CRT_IMAD && engine != NC_CRT_TC_I8) throw nc::Error(nc::kEInval, "unknown CRT engine");
+        if (engine == NC_CRT_TC_I8 && !plan->p->d_crt_b)
+            throw nc::Error(nc::kEInval, "the tensor-core CRT takes at most 32 primes (q up to about 960 bits)");
+        plan->p->crt_tc = engine == NC_CRT_TC_I8;
+    });
+}
+
+int nc_plan_get_crt_engine(const nc_plan* plan) {
+    if (!plan) {
+        nc::set_last_error("null plan");
+        return NC_EINVAL;
+    }
+    return (plan->p->crt_tc && plan->p->d_crt_b) ? NC_CRT_TC_I8 : NC_CRT_IMAD;
+}
+
 int nc_plan_synchronize(nc_plan* plan) {
     return guarded([&] {
         if (!plan) throw nc::Error(nc::kEInval, "null plan");

@@ -73,6 +73,7 @@ struct ProductDesc {
     uint32_t k;
     uint32_t mode;          // kModeProduct, kModeCachedA, kModeForward
     uint32_t logN2;         // row block size of the row configuration (N1 = N >> logN2)
+    const uint4* crt_b;     // the plan's byte table for the tensor-core CRT (null: integer-pipe CRT)
 };
 
 enum : uint32_t { kModeProduct = 0, kModeCachedA = 1, kModeForward = 2 };
@@ -98,6 +99,21 @@ NC_HD constexpr size_t crt_smem_bytes(int k) {
            + size_t(k) * kMqStride * 4                                       // M/p_i mod q
            + size_t(k) * 8 * 3                                               // y, y shoup, p
            + size_t(kMqStride) * 4 * 2 + 16;                                 // -M mod q, q, mu
+}
+
+// Tensor-core CRT (plain path): a 256-coefficient tile is two 128-row halves of A, each 128 rows x
+// 256 K bytes (8 bytes of v_i per prime, so at most 32 primes); the plan's table B has NC output
+// byte columns (4 LW + 7 rounded up to 16) x 256 K bytes.
+constexpr int kCrtTcMaxPrimes = 32;
+constexpr int kCrtTcHalfBytes = 128 * 256;
+NC_HD constexpr int crt_tc_cols(int LW) { return (4 * LW + 7 + 15) / 16 * 16; }
+NC_HD constexpr size_t crt_tc_table_bytes(int LW) { return size_t(crt_tc_cols(LW)) * 256; }
+// Operands, constants, mbarrier and tensor-memory slot; raised so that no more CTAs share an SM
+// than its 512 tensor-memory columns hold (two accumulators of NC columns, rounded up to 256 or 512).
+NC_HD constexpr size_t crt_tc_smem_bytes(int LW) {
+    return smax(size_t(2) * kCrtTcHalfBytes + crt_tc_table_bytes(LW) + size_t(kCrtTcMaxPrimes) * 8 * 3 +
+                    size_t(kMqStride) * 4 * 2 + 16 + 16,
+                (size_t(233472) / (512 / (2 * crt_tc_cols(LW) <= 256 ? 256 : 512) + 1) + 16) / 16 * 16);
 }
 
 // How the row stage tiles a product: row blocks of N2 = 2^logN2 residues, each thread holding

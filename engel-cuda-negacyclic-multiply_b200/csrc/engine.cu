@@ -160,8 +160,33 @@ ProductDesc Plan::desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const 
     d.k = uint32_t(k);
     d.mode = kModeProduct;
     d.logN2 = uint32_t(cfg.logN2);
+    d.crt_b = crt_tc ? d_crt_b : nullptr;
     return d;
 }
+
+namespace {
+
+// Table B of the tensor-core CRT in the MMA's shared-memory order: output byte column c, K byte
+// 8 i + a holds byte c - a of (M/p_i) mod q (zero outside 0 <= c - a < 4 L), stored at
+// (c / 8) * 2048 + (K / 16) * 128 + (c % 8) * 16 + K % 16.
+std::vector<uint8_t> crt_tc_table(const QConst& hq) {
+    const int LW = int(hq.LW), L = int(hq.L), k = int(hq.k);
+    const int NC = crt_tc_cols(LW);
+    std::vector<uint8_t> b(crt_tc_table_bytes(LW), 0);
+    for (int c = 0; c < NC; ++c)
+        for (int i = 0; i < k; ++i)
+            for (int a = 0; a < 8; ++a) {
+                const int byte = c - a;
+                if (byte < 0 || byte >= 4 * L) continue;
+                const uint32_t word = hq.mq[size_t(i) * kMqStride + size_t(byte / 4)];
+                const int K = 8 * i + a;
+                b[size_t(c / 8) * 2048 + size_t(K / 16) * 128 + size_t(c % 8) * 16 + size_t(K % 16)] =
+                    uint8_t(word >> (8 * (byte % 4)));
+            }
+    return b;
+}
+
+}  // namespace
 
 static int copy_threads() {
     if (const char* s = std::getenv("NC_COPY_THREADS")) {
@@ -203,6 +228,13 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
         // ordered on the plan's stream and complete before any other stream can use the plan
         check(cudaMemcpyAsync(p->d_qc, &p->hq, sizeof(QConst), cudaMemcpyHostToDevice, p->stream),
               "plan constants upload");
+        std::vector<uint8_t> crt_b;
+        if (p->k <= kCrtTcMaxPrimes) {
+            crt_b = crt_tc_table(p->hq);
+            check(cudaMalloc(&p->d_crt_b, crt_b.size()), "CRT table");
+            check(cudaMemcpyAsync(p->d_crt_b, crt_b.data(), crt_b.size(), cudaMemcpyHostToDevice, p->stream),
+                  "CRT table upload");
+        }
         check(cudaStreamSynchronize(p->stream), "plan constants upload");
         check(cudaEventCreate(&p->ev_start), "event");
         check(cudaEventCreate(&p->ev_stop), "event");
@@ -257,6 +289,7 @@ void plan_destroy(Plan* p) {
     if (p->ev_a) cudaEventDestroy(p->ev_a);
     if (p->ev_b) cudaEventDestroy(p->ev_b);
     cudaFree(p->d_qc);
+    cudaFree(p->d_crt_b);
     cudaFree(p->d_ra);
     cudaFree(p->d_rb);
     cudaFree(p->d_a);

@@ -48,6 +48,7 @@ cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32) {
     cudaError_t e = prepare_dec(pc, pow32);
     if (e == cudaSuccess) e = prepare_row(pc, pow32);
     if (e == cudaSuccess) e = prepare_crt(pc, pow32);
+    if (e == cudaSuccess) e = prepare_crt_tc(pc, pow32);
     if (e == cudaSuccess) e = prepare_persistent(pc, pow32);
     if (e == cudaSuccess) e = prepare_residues(pc, pow32);
     return e;
@@ -58,7 +59,7 @@ cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfi
     if (int(d.logN2) != cfg.logN2) return cudaErrorInvalidValue;
     void* row = row_kernel(cfg);
     void* dec = dec_kernel(int(d.LW));
-    void* crt = crt_kernel(int(d.LW));
+    void* crt = d.crt_b ? crt_tc_kernel(int(d.LW)) : crt_kernel(int(d.LW));
     if (!row || !dec || !crt) return cudaErrorInvalidValue;
     const Geometry g = geometry(int(d.logN), int(d.k), cfg);
     ProductDesc dd = d;
@@ -90,7 +91,8 @@ cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfi
     if (ev && (e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
     if (d.mode != kModeForward) {
         void* args[] = {&dd, &tt};
-        e = launch(crt, g.tiles, kThreads, crt_smem_bytes(int(d.k)), s, args);
+        e = launch(crt, g.tiles, kThreads, d.crt_b ? crt_tc_smem_bytes(int(d.LW)) : crt_smem_bytes(int(d.k)), s,
+                   args);
         if (e != cudaSuccess) return e;
     }
     if (ev && (e = cudaEventRecord(ev[3], s)) != cudaSuccess) return e;

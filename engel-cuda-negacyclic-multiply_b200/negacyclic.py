@@ -34,6 +34,8 @@ C_SYMBOLS = [
     ("nc_multiply", ctypes.c_int, [_vp, _u32p, _u32p, _u32p]),
     ("nc_multiply_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     ("nc_multiply_device_noalloc", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    ("nc_plan_set_crt_engine", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nc_plan_get_crt_engine", ctypes.c_int, [_vp]),
     ("nc_plan_synchronize", ctypes.c_int, [_vp]),
     ("nc_plan_query", ctypes.c_int, [_vp, _u32p, _u32p, _u32p, _u32p]),
     ("nc_plan_last_kernel_ms", ctypes.c_float, [_vp]),
@@ -121,6 +123,7 @@ def primes(count: int = 48) -> list[int]:
 
 
 RESIDUES_IMAD, RESIDUES_TC_I8 = 0, 1
+CRT_IMAD, CRT_TC_I8 = 0, 1
 
 
 def residues_gave_up() -> bool:
@@ -171,6 +174,18 @@ class Plan:
         """Residue stage alone (an ablation): d_r[i * N + n] = x_n mod p_i, k * N u64, by the integer
         pipes (RESIDUES_IMAD) or an exact INT8 tensor-core contraction (RESIDUES_TC_I8)."""
         _check(load().nc_residues(self._h, _vp(d_x), _vp(d_r), int(engine), _vp(stream or None)))
+
+    @property
+    def crt_engine(self) -> int:
+        """CRT_TC_I8 (tensor cores, the default for <= 32 primes) or CRT_IMAD (integer pipes)."""
+        v = load().nc_plan_get_crt_engine(self._h)
+        if v < 0:
+            _check(v)
+        return v
+
+    @crt_engine.setter
+    def crt_engine(self, engine: int) -> None:
+        _check(load().nc_plan_set_crt_engine(self._h, int(engine)))
 
     def synchronize(self) -> None:
         _check(load().nc_plan_synchronize(self._h))

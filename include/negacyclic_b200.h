@@ -68,6 +68,20 @@ int nc_multiply_device(nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, 
 int nc_multiply_device_noalloc(const nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
                                void* stream);
 
+/* Engine of the CRT accumulation sum_i v_i (M/p_i mod q) on the plan's plain path (the counterpart
+   of fast_crt_kernel's 34-limb multiply-adds, solve.cu:752-836):
+     NC_CRT_TC_I8  the default when the plan has at most 32 primes (q up to about 960 bits): an exact
+                   u8 x u8 contraction of the bytes of v_i with a per-plan table of the bytes of
+                   M/p_i mod q on the tensor cores (tcgen05.mma kind::i8, s32 accumulators in tensor
+                   memory), folded back into limbs with one carry pass;
+     NC_CRT_IMAD   the same sum as 32-bit carry chains on the integer pipes (always available; batches
+                   and servers use it).
+   Both give the same integer and so the same product. Set it only while no product of the plan
+   is in flight. nc_plan_get_crt_engine returns the engine in use. */
+enum { NC_CRT_IMAD = 0, NC_CRT_TC_I8 = 1 };
+int nc_plan_set_crt_engine(nc_plan* plan, int engine);
+int nc_plan_get_crt_engine(const nc_plan* plan);
+
 /* Waits for the plan's own stream (the one nc_multiply uses). */
 int nc_plan_synchronize(nc_plan* plan);
 
