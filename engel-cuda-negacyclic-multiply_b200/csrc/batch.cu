@@ -1,4 +1,4 @@
-// Batches of products run by one persistent kernel launch (host side; see batch.h).
+// Batches of products: one persistent launch for residues and rows, then the CRT launches (host side).
 #include "batch.h"
 
 #include <algorithm>
@@ -99,7 +99,8 @@ void Batch::finalize(cudaStream_t stream) {
         check(cudaMalloc(&scratch_, scratch), "batch scratch");
         scratch_bytes_ = scratch;
     }
-    std::vector<uint2> dec, row, crt;
+    std::vector<uint2> dec, row, crt, crt_tc;
+    int lw_tc = 2;
     size_t off = 0;
     char* base = reinterpret_cast<char*>(scratch_);
     for (size_t p = 0; p < n; ++p) {
@@ -130,16 +131,25 @@ void Batch::finalize(cudaStream_t stream) {
         const uint32_t pid = uint32_t(p);
         for (uint32_t i = 0; i < bp.n_dec; ++i) dec.push_back(make_uint2((kItemDec << 28) | pid, i));
         for (uint32_t i = 0; i < bp.n_row; ++i) row.push_back(make_uint2((kItemRow << 28) | pid, i));
-        if (e.mode != kModeForward)
-            for (uint32_t i = 0; i < uint32_t(g.tiles); ++i) crt.push_back(make_uint2((kItemCrt << 28) | pid, i));
+        if (e.mode != kModeForward) {
+            // CRT on the tensor cores for products with a table and at most 30 limbs
+            const bool tc = d.crt_b && crt_tc_tmem_cols(int(d.LW)) == 256;
+            if (tc) lw_tc = std::max(lw_tc, int(d.LW));
+            for (uint32_t i = 0; i < uint32_t(g.tiles); ++i) (tc ? crt_tc : crt).push_back(make_uint2(pid, i));
+        }
         shape.push_back((uint64_t(pl->logN) << 40) | (uint64_t(pl->k) << 32) | (uint64_t(pl->L) << 8) | e.mode);
     }
+    // queue of the persistent launch (residue, then row items), then the two CRT item lists
     std::vector<uint2> items;
-    items.reserve(dec.size() + row.size() + crt.size());
+    items.reserve(dec.size() + row.size() + crt_tc.size() + crt.size());
     items.insert(items.end(), dec.begin(), dec.end());
     items.insert(items.end(), row.begin(), row.end());
-    items.insert(items.end(), crt.begin(), crt.end());
     n_items_ = int(items.size());
+    n_crt_tc_ = int(crt_tc.size());
+    n_crt_ = int(crt.size());
+    items.insert(items.end(), crt_tc.begin(), crt_tc.end());
+    items.insert(items.end(), crt.begin(), crt.end());
+    shape.push_back((uint64_t(n_crt_tc_) << 32) | uint64_t(lw_tc));
 
     ensure(reinterpret_cast<char**>(&d_products_), &products_cap_, n * sizeof(BatchProduct), "batch products");
     ensure(&d_items_, &items_cap_, items.size(), "batch items");
@@ -168,7 +178,9 @@ void Batch::finalize(cudaStream_t stream) {
         check(cudaMemcpyAsync(d_items_, h_upload_ + prod_bytes, item_bytes, cudaMemcpyHostToDevice, stream), "upload");
     }
 
-    smem_ = smax(smax(dec_smem_bytes(kmax), crt_smem_bytes(kmax)), row_smem_bytes(kThreads, 4));
+    smem_ = smax(dec_smem_bytes(kmax), row_smem_bytes(kThreads, 4));
+    smem_crt_ = crt_smem_bytes(kmax);
+    smem_crt_tc_ = crt_tc_smem_bytes(lw_tc);
     int per_sm = 0, sms = 0;
     check(persistent_occupancy(smem_, &per_sm), "occupancy");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "device attribute");
@@ -195,10 +207,24 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
     args.head = d_state_ + 2 * n;
     args.error = d_state_ + 2 * n + 1;
     args.tables = tables_->view();
+    BatchCrtArgs tc{}, im{};
+    tc.products = im.products = args.products;
+    tc.tables = im.tables = args.tables;
+    tc.items = d_items_ + n_items_;
+    tc.n_items = n_crt_tc_;
+    im.items = d_items_ + n_items_ + n_crt_tc_;
+    im.n_items = n_crt_;
+    // the persistent launch, then the CRT launches (every row item is done when they start)
+    auto enqueue = [&](cudaStream_t s) -> cudaError_t {
+        cudaError_t e = launch_persistent(args, ctas_, smem_, s);
+        if (e == cudaSuccess && n_crt_tc_ > 0) e = launch_batch_crt(tc, true, smem_crt_tc_, s);
+        if (e == cudaSuccess && n_crt_ > 0) e = launch_batch_crt(im, false, smem_crt_, s);
+        return e;
+    };
     const size_t state_bytes = (2 * n + 5) * sizeof(uint32_t);
     if (!use_graph) {
         check(cudaMemsetAsync(d_state_, 0, state_bytes, stream), "batch reset");
-        check(launch_persistent(args, ctas_, smem_, stream), "persistent launch");
+        check(enqueue(stream), "batch launch");
         check(cudaMemcpyAsync(err_host_, args.error, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream), "batch status");
         check(cudaEventRecord(done_, stream), "batch event");
         ran_ = true;
@@ -210,8 +236,9 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
         cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             cudaMemsetAsync(d_state_, 0, state_bytes, cap);
-            launch_persistent(args, ctas_, smem_, cap);
+            const cudaError_t le = enqueue(cap);
             e = cudaStreamEndCapture(cap, &graph_);
+            if (e == cudaSuccess) e = le;
         }
         cudaStreamDestroy(cap);
         check(e, "graph capture");

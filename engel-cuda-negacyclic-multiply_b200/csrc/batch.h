@@ -1,4 +1,4 @@
-// Batches of products run by one persistent kernel launch (host side).
+// Batches of products: one persistent launch for residues and rows, then the CRT launches (host side).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -13,9 +13,10 @@ namespace nc {
 
 
 // A list of products (each referring to a plan for its q, N and constants) that run together.
-// Products may differ in N and in q. Residue scratch comes from the batch's own arena; the
-// counter reset and the launch are captured once into a CUDA graph and replayed while the
-// batch keeps the same shape.
+// Products may differ in N and in q. Residue scratch comes from the batch's own arena. A run is
+// one persistent launch for the residue and row stages of every product, then one CRT launch per
+// CRT engine in use; the counter reset and the launches are captured once into a CUDA graph and
+// replayed while the batch keeps the same shape.
 class Batch {
   public:
     explicit Batch(int device);
@@ -35,7 +36,7 @@ class Batch {
     void synchronize();
     int ctas() const { return ctas_; }
     size_t scratch_bytes() const { return scratch_bytes_; }
-    int launches_per_run() const { return 1; }
+    int launches_per_run() const { return 1 + (n_crt_tc_ > 0 ? 1 : 0) + (n_crt_ > 0 ? 1 : 0); }
     // After the last run has completed (its event): did a dependency wait give up?
     bool failed() const;
     // What the failed wait waited for (empty when nothing failed).
@@ -69,7 +70,10 @@ class Batch {
     size_t scratch_bytes_ = 0;
     int n_items_ = 0;
     int ctas_ = 0;
-    size_t smem_ = 0;
+    size_t smem_ = 0;      // persistent launch (residue and row items)
+    int n_crt_tc_ = 0;     // CRT items on the tensor cores, after the persistent queue in d_items_
+    int n_crt_ = 0;        // CRT items on the integer pipes, after those
+    size_t smem_crt_tc_ = 0, smem_crt_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
     cudaEvent_t done_ = nullptr;  // recorded after every run

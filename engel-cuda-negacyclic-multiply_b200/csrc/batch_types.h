@@ -22,11 +22,19 @@ struct BatchProduct {
 
 struct BatchArgs {
     const BatchProduct* products;
-    const uint2* items;  // x = stage << 28 | product, y = index inside the stage
+    const uint2* items;  // x = stage << 28 | product, y = index inside the stage (residue and row items)
     int n_items;
     uint32_t* counters;  // per product: residue items done, row items done
     uint32_t* head;      // next queue position
     uint32_t* error;     // [0] nonzero once a wait gave up; [1..3] what it waited for
+    Tables tables;
+};
+
+// The CRT launches of a batch: one CTA per item (x = product, y = 256-coefficient tile).
+struct BatchCrtArgs {
+    const BatchProduct* products;
+    const uint2* items;
+    int n_items;
     Tables tables;
 };
 

@@ -108,12 +108,14 @@ constexpr int kCrtTcMaxPrimes = 32;
 constexpr int kCrtTcHalfBytes = 128 * 256;
 NC_HD constexpr int crt_tc_cols(int LW) { return (4 * LW + 7 + 15) / 16 * 16; }
 NC_HD constexpr size_t crt_tc_table_bytes(int LW) { return size_t(crt_tc_cols(LW)) * 256; }
-// Operands, constants, mbarrier and tensor-memory slot; raised so that no more CTAs share an SM
+// tensor-memory columns of one tile: two accumulators of NC columns, rounded up to 256 or 512
+NC_HD constexpr uint32_t crt_tc_tmem_cols(int LW) { return 2 * crt_tc_cols(LW) <= 256 ? 256u : 512u; }
+// Operands and constants; raised so that no more CTAs share an SM
 // than its 512 tensor-memory columns hold (two accumulators of NC columns, rounded up to 256 or 512).
 NC_HD constexpr size_t crt_tc_smem_bytes(int LW) {
     return smax(size_t(2) * kCrtTcHalfBytes + crt_tc_table_bytes(LW) + size_t(kCrtTcMaxPrimes) * 8 * 3 +
                     size_t(kMqStride) * 4 * 2 + 16 + 16,
-                (size_t(233472) / (512 / (2 * crt_tc_cols(LW) <= 256 ? 256 : 512) + 1) + 16) / 16 * 16);
+                (size_t(233472) / (512 / crt_tc_tmem_cols(LW) + 1) + 16) / 16 * 16);
 }
 
 // How the row stage tiles a product: row blocks of N2 = 2^logN2 residues, each thread holding

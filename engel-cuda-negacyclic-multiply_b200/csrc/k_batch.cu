@@ -1,13 +1,20 @@
-// Persistent batched kernel: every product of a batch, in one launch.
+// Batched kernels: every product of a batch in one persistent launch for the residue and row
+// stages, then the CRT stage of every product in one launch per CRT engine.
 //
-// The host lays out a work queue of items (stage, product, index): all residue items of every
-// product, then all row items, then all CRT items. CTAs (as many as fit on the GPU at once)
-// take items in queue order with one atomic. A row item of product p may start once every
-// residue item of p is done, a CRT item once every row item of p is done; the CTA's first
-// thread polls p's counter. Every item a CTA waits for was taken earlier by a CTA that is
-// running and waits on nothing later in the queue, so the waits always end. A wait is still
-// bounded: past kSpinLimit polls (about two seconds) the CTA records an error, skips the
-// item, and every later wait returns at once; the host reports the error after the launch.
+// Persistent launch: the host lays out a work queue of items (stage, product, index): all residue
+// items of every product, then all row items. CTAs (as many as fit on the GPU at once) take items
+// in queue order with one atomic. A row item of product p may start once every residue item of p
+// is done; the CTA's first thread polls p's counter. Every item a CTA waits for was taken earlier
+// by a CTA that is running and waits on nothing later in the queue, so the waits always end. A
+// wait is still bounded: past kSpinLimit polls (about two seconds) the CTA records an error, skips
+// the item, and every later wait returns at once; the host reports the error after the launch.
+//
+// CRT launches (after the persistent launch on the same stream, so every row item is done): one
+// CTA per (product, 256-coefficient tile). Products with a tensor-core table and at most 30 limbs
+// run crt_coeffs_tc in k_batch_crt_tc (256 tensor-memory columns per CTA); the others run
+// crt_coeffs in k_batch_crt. Keeping the CRT out of the persistent loop keeps its register-heavy
+// code out of the residue and row items' register allocation.
+#include "crt_tc.cuh"
 #include "kernel_registry.h"
 #include "stages.cuh"
 
@@ -65,14 +72,6 @@ __device__ __forceinline__ void batch_item(uint32_t stage, const BatchProduct& b
 #undef NC_B_ROW
             default: break;
         }
-    } else {
-        switch (bp.d.LW) {
-#define NC_B_CRT(n) \
-    case n: crt_coeffs<n>(bp.d, t, idx, smem); break;
-            NC_LW_CASES(NC_B_CRT)
-#undef NC_B_CRT
-            default: break;
-        }
     }
 }
 
@@ -92,7 +91,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
         if (threadIdx.x == 0) {
             bool ok = true;
             if (stage == kItemRow) ok = wait_count(a.counters + 2 * prod, bp.n_dec, a.error, w.x);
-            if (stage == kItemCrt) ok = wait_count(a.counters + 2 * prod + 1, bp.n_row, a.error, w.x);
             s_go = ok ? 1 : 0;
         }
         __syncthreads();
@@ -100,18 +98,79 @@ __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
             batch_item(stage, bp, a.tables, int(w.y), smem);
             __threadfence();
             __syncthreads();
-            if (threadIdx.x == 0 && stage != kItemCrt) atomicAdd(a.counters + 2 * prod + stage, 1u);
+            if (threadIdx.x == 0 && stage == kItemDec) atomicAdd(a.counters + 2 * prod, 1u);
         }
         __syncthreads();  // s_item / s_go are rewritten by the next round
     }
 }
 
+__global__ void __launch_bounds__(kThreads, 2) k_batch_crt(BatchCrtArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const uint2 w = __ldg(a.items + blockIdx.x);
+    const BatchProduct& bp = a.products[w.x];
+    switch (bp.d.LW) {
+#define NC_B_CRT(n) \
+    case n: crt_coeffs<n>(bp.d, a.tables, int(w.y), smem); break;
+        NC_LW_CASES(NC_B_CRT)
+#undef NC_B_CRT
+        default: break;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) k_batch_crt_tc(BatchCrtArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t taddr_slot;
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(
+                         crt_tc_detail::smem_u32(&taddr_slot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(crt_tc_detail::smem_u32(&bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t taddr = taddr_slot;
+    const uint2 w = __ldg(a.items + blockIdx.x);
+    const BatchProduct& bp = a.products[w.x];
+    switch (bp.d.LW) {
+#define NC_B_CRT_TC(n)                                                        \
+    case n:                                                                   \
+        if constexpr (crt_tc_tmem_cols(n) == 256)                             \
+            crt_coeffs_tc<n>(bp.d, a.tables, int(w.y), smem, taddr, &bar, 0); \
+        break;
+        NC_LW_CASES(NC_B_CRT_TC)
+#undef NC_B_CRT_TC
+        default: break;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(taddr) : "memory");
+}
+
+cudaError_t launch_batch_crt(const BatchCrtArgs& args, bool tensor_cores, size_t smem, cudaStream_t s) {
+    BatchCrtArgs a = args;
+    void* params[] = {&a};
+    void* fn = tensor_cores ? reinterpret_cast<void*>(&k_batch_crt_tc) : reinterpret_cast<void*>(&k_batch_crt);
+    return cudaLaunchKernel(fn, dim3(unsigned(args.n_items)), dim3(kThreads), params, smem, s);
+}
+
 cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
     cudaError_t e = upload_prime_constants(pc, pow32);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(smax(smax(dec_smem_bytes(kMaxPrimes), crt_smem_bytes(kMaxPrimes)),
-                                         row_smem_bytes(kThreads, 4))));
+    e = cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(smax(dec_smem_bytes(kMaxPrimes), row_smem_bytes(kThreads, 4))));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_crt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(crt_smem_bytes(kMaxPrimes)));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_crt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(crt_tc_smem_bytes(30)));
+    return e;
 }
 
 // Launch with `ctas` persistent CTAs and `smem` dynamic shared memory.

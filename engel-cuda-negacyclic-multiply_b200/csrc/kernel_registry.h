@@ -25,6 +25,7 @@ cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32);
 cudaError_t prepare_residues(const PrimeConst* pc, const uint64_t* pow32);
 
 cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s);
+cudaError_t launch_batch_crt(const BatchCrtArgs& args, bool tensor_cores, size_t smem, cudaStream_t s);
 cudaError_t persistent_occupancy(size_t smem, int* ctas_per_sm);
 
 }  // namespace nc
