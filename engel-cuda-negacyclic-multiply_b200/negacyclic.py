@@ -252,7 +252,8 @@ def row_variants(log_n: int) -> list[tuple[int, int, int]]:
 
 
 class Batch:
-    """Many products (any mix of plans) in one persistent launch (nc_batch_*). Device pointers."""
+    """Many products (any mix of plans) in one persistent launch for residues and rows plus one CRT
+    launch per engine (nc_batch_*). Device pointers."""
 
     def __init__(self):
         self._h = _vp()

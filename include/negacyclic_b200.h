@@ -74,8 +74,8 @@ int nc_multiply_device_noalloc(const nc_plan* plan, const uint32_t* d_a, const u
                    u8 x u8 contraction of the bytes of v_i with a per-plan table of the bytes of
                    M/p_i mod q on the tensor cores (tcgen05.mma kind::i8, s32 accumulators in tensor
                    memory), folded back into limbs with one carry pass;
-     NC_CRT_IMAD   the same sum as 32-bit carry chains on the integer pipes (always available; batches
-                   and servers use it).
+     NC_CRT_IMAD   the same sum as 32-bit carry chains on the integer pipes (always available).
+   Batches and servers follow the plan's engine (tensor cores for plans of at most 30 limbs).
    Both give the same integer and so the same product. Set it only while no product of the plan
    is in flight. nc_plan_get_crt_engine returns the engine in use. */
 enum { NC_CRT_IMAD = 0, NC_CRT_TC_I8 = 1 };
@@ -142,11 +142,12 @@ int nc_plan_autotune(nc_plan* plan, int reps, float* best_ms);
 
 /* ------------------------------------------------------------------ batches
  *
- * A batch runs many products, of any mix of N and q (one plan each), in ONE persistent kernel
- * launch: per-(prime, row block) and per-tile work items in a global queue, dependency
- * counters per product, bounded waits. The counter reset and the launch are captured into a
- * CUDA graph and replayed while the batch keeps its shape. Device buffers are 16-byte aligned
- * and must stay valid until the batch has run. */
+ * A batch runs many products, of any mix of N and q (one plan each), in one persistent kernel
+ * launch for the residue and row stages (per-tile and per-(prime, row block) work items in a
+ * global queue, dependency counters per product, bounded waits), followed by one CRT launch per
+ * CRT engine in use (one CTA per product tile). The counter reset and the launches are captured
+ * into a CUDA graph and replayed while the batch keeps its shape. Device buffers are 16-byte
+ * aligned and must stay valid until the batch has run. */
 
 typedef struct nc_batch nc_batch;
 

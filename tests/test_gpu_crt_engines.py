@@ -47,3 +47,36 @@ def test_tensor_engine_unavailable_beyond_32_primes(gpu):
         with pytest.raises(nc.NegacyclicError) as ei:
             plan.crt_engine = nc.CRT_TC_I8
         assert ei.value.code == nc.NC_EINVAL
+
+
+def test_batch_mixes_both_crt_engines(gpu):
+    """One batch with tensor-core CRT items (868-bit), integer CRT items (1000-bit: 33 primes) and a
+    plan switched to the integer engine: every product matches the oracle."""
+    import torch
+
+    specs = [(4096, 868, nc.CRT_TC_I8), (2048, 1000, None), (8192, 868, nc.CRT_IMAD), (1024, 434, nc.CRT_TC_I8)]
+    plans, bufs, want = [], [], []
+    try:
+        for i, (N, bits, engine) in enumerate(specs):
+            c = cases.make_case(N, bits, seed=600 + i, edge_frac=0.02)
+            p = nc.Plan(N, c.q_limbs, W=c.W)
+            if engine is not None:
+                p.crt_engine = engine
+            else:
+                assert p.crt_engine == nc.CRT_IMAD
+            plans.append(p)
+            x = torch.from_numpy(c.a.view(np.int32).copy()).cuda()
+            y = torch.from_numpy(c.b.view(np.int32).copy()).cuda()
+            bufs.append((x, y, torch.empty_like(x)))
+            want.append(oracle.negacyclic(N, c.q_limbs, c.a, c.b))
+        with nc.Batch() as batch:
+            for p, (x, y, z) in zip(plans, bufs):
+                batch.add(p, x.data_ptr(), y.data_ptr(), z.data_ptr())
+            for use_graph in (False, True, True):
+                batch.run(0, use_graph)
+                batch.synchronize()
+                for (_, _, z), w in zip(bufs, want):
+                    assert np.array_equal(z.cpu().numpy().view(np.uint32).reshape(w.shape), w)
+    finally:
+        for p in plans:
+            p.close()
