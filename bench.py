@@ -329,7 +329,9 @@ def ours(args) -> dict | None:
     work = stage_work(k, N, L)
     sbytes = stage_bytes(k, N, L)
     dom = max(range(3), key=lambda i: mean_stage[i])
-    names = ["residues+forward columns", "row NTTs+pointwise", "inverse columns+CRT"]
+    crt_tc = plan.crt_engine == nc.CRT_TC_I8
+    names = ["residues+forward columns", "row NTTs+pointwise",
+             "inverse columns+CRT (accumulation on the tensor cores)" if crt_tc else "inverse columns+CRT"]
     kernels = ["k_dec", "k_row", "k_crt"]
     traffic = None
     if TRAFFIC_FILE.exists():
