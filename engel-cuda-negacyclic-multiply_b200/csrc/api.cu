@@ -81,6 +81,38 @@ int nc_multiply_device(nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, 
     });
 }
 
+int nc_plan_create_chain(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int factors, nc_plan** out) {
+    return guarded([&] {
+        if (!out) throw nc::Error(nc::kEInval, "out is null");
+        *out = nullptr;
+        if (factors < 2 || factors > nc::kMaxFactors) throw nc::Error(nc::kEInval, "factors must be 2, 3 or 4");
+        nc::Plan* p = nc::plan_create(N, W, L, q, factors);
+        *out = new nc_plan{p};
+    });
+}
+
+int nc_plan_factors(const nc_plan* plan) {
+    if (!plan) {
+        nc::set_last_error("null plan");
+        return NC_EINVAL;
+    }
+    return plan->p->factors;
+}
+
+int nc_multiply_chain(nc_plan* plan, const uint32_t* const* x, uint32_t* c) {
+    return guarded([&] {
+        if (!plan) throw nc::Error(nc::kEInval, "null plan");
+        nc::plan_multiply_chain_host(plan->p, x, c);
+    });
+}
+
+int nc_multiply_chain_device(nc_plan* plan, const uint32_t* const* d_x, uint32_t* d_c, void* stream) {
+    return guarded([&] {
+        if (!plan) throw nc::Error(nc::kEInval, "null plan");
+        nc::plan_multiply_chain_device(plan->p, d_x, d_c, static_cast<cudaStream_t>(stream));
+    });
+}
+
 int nc_plan_set_crt_engine(nc_plan* plan, int engine) {
     return guarded([&] {
         if (!plan) throw nc::Error(nc::kEInval, "null plan");

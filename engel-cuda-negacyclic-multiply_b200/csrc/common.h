@@ -31,6 +31,7 @@ constexpr int kTile = 256;           // coefficients per decomposition / CRT til
 constexpr int kRowLogMax = 12;       // a row block holds at most 4096 residues (32 KB)
 constexpr int kAccExtra = 3;         // CRT accumulator words beyond q's limbs (acc < 2^(bits(q)+69))
 constexpr int kBarrettT = 69;        // acc < 2^(bits(q) + kBarrettT)
+constexpr int kMaxFactors = 4;       // a chained product multiplies 2 to 4 operands in one pass
 
 // Per-prime constants. p = 2^62 - m, m < 2^28 for all primes of the set.
 struct PrimeConst {
@@ -74,7 +75,18 @@ struct ProductDesc {
     uint32_t mode;          // kModeProduct, kModeCachedA, kModeForward
     uint32_t logN2;         // row block size of the row configuration (N1 = N >> logN2)
     const uint4* crt_b;     // the plan's byte table for the tensor-core CRT (null: integer-pipe CRT)
+    uint32_t factors;       // operands of the product (2: a b; 3, 4: a b x_more[0] [x_more[1]])
+    const uint32_t* x_more[kMaxFactors - 2];  // further operands (N x L limbs)
+    uint64_t* r_more[kMaxFactors - 2];        // their residues (k x N scratch)
 };
+
+// Operand f of a product (0: a, 1: b, 2..: x_more) and its residue buffer.
+NC_HD inline const uint32_t* factor_limbs(const ProductDesc& d, int f) {
+    return f == 0 ? d.a : f == 1 ? d.b : d.x_more[f - 2];
+}
+NC_HD inline uint64_t* factor_residues(const ProductDesc& d, int f) {
+    return f == 0 ? d.ra : f == 1 ? d.rb : d.r_more[f - 2];
+}
 
 enum : uint32_t { kModeProduct = 0, kModeCachedA = 1, kModeForward = 2 };
 

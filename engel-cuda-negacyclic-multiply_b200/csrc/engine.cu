@@ -161,6 +161,17 @@ ProductDesc Plan::desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const 
     d.mode = kModeProduct;
     d.logN2 = uint32_t(cfg.logN2);
     d.crt_b = crt_tc ? d_crt_b : nullptr;
+    d.factors = 2;
+    return d;
+}
+
+ProductDesc Plan::desc_chain(const uint32_t* const* x, uint32_t* c) const {
+    ProductDesc d = desc(x[0], x[1], c);
+    d.factors = uint32_t(factors);
+    for (int f = 2; f < factors; ++f) {
+        d.x_more[f - 2] = x[f];
+        d.r_more[f - 2] = d_rx[f - 2];
+    }
     return d;
 }
 
@@ -197,7 +208,7 @@ static int copy_threads() {
     return hc < 2 ? 1 : (hc < 8 ? hc : 8);
 }
 
-Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
+Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int factors) {
     if (N < 2 || N > uint32_t(kMaxN) || (N & (N - 1)) != 0)
         throw Error(kEInval, "N must be a power of two from 2 to 65536");
     if (L == 0 || L > uint32_t(kMaxL)) throw Error(kEInval, "L must be between 1 and 32");
@@ -208,7 +219,8 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
     p->N = int(N);
     p->L = int(L);
     p->logN = logN;
-    const std::string err = build_qconst(q, int(L), logN, &p->hq);
+    p->factors = factors;
+    const std::string err = build_qconst(q, int(L), logN, &p->hq, factors);
     if (!err.empty()) {
         delete p;
         throw Error(kEInval, err);
@@ -251,13 +263,17 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
 void ensure_scratch(Plan* p) {
     if (p->d_ra) return;
     const size_t res = size_t(p->k) * p->N * sizeof(uint64_t);
-    check(cudaMalloc(&p->d_ra, res), "residues a");
-    const cudaError_t e = cudaMalloc(&p->d_rb, res);
-    if (e != cudaSuccess) {
-        cudaFree(p->d_ra);
-        p->d_ra = nullptr;
-        check(e, "residues b");
+    uint64_t* bufs[kMaxFactors] = {};
+    for (int f = 0; f < p->factors; ++f) {
+        const cudaError_t e = cudaMalloc(&bufs[f], res);
+        if (e != cudaSuccess) {
+            for (int g = 0; g < f; ++g) cudaFree(bufs[g]);
+            check(e, "residue scratch");
+        }
     }
+    p->d_rb = bufs[1];
+    for (int f = 2; f < p->factors; ++f) p->d_rx[f - 2] = bufs[f];
+    p->d_ra = bufs[0];
 }
 
 // Staging for host operands (device copies, pinned buffers, copy threads), on first use.
@@ -271,6 +287,10 @@ void ensure_host_path(Plan* p) {
     check(cudaMallocHost(&p->h_a, limbs), "pinned a");
     check(cudaMallocHost(&p->h_b, limbs), "pinned b");
     check(cudaMallocHost(&p->h_c, limbs), "pinned c");
+    for (int f = 2; f < p->factors; ++f) {
+        check(cudaMalloc(&p->d_x[f - 2], limbs), "input operand");
+        check(cudaMallocHost(&p->h_x[f - 2], limbs), "pinned operand");
+    }
     // one set of copy threads per process, shared by every plan (jobs run one at a time)
     static HostPool* shared = new HostPool(copy_threads());
     p->ev_out.assign(size_t(shared->parts()), nullptr);
@@ -292,6 +312,11 @@ void plan_destroy(Plan* p) {
     cudaFree(p->d_crt_b);
     cudaFree(p->d_ra);
     cudaFree(p->d_rb);
+    for (int f = 0; f < kMaxFactors - 2; ++f) {
+        cudaFree(p->d_rx[f]);
+        cudaFree(p->d_x[f]);
+        cudaFreeHost(p->h_x[f]);
+    }
     cudaFree(p->d_a);
     cudaFree(p->d_b);
     cudaFree(p->d_c);
@@ -346,9 +371,13 @@ int out_chunks(size_t bytes, int parts, size_t* chunk) {
 
 }  // namespace
 
-void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
+namespace {
+
+// Host operands x[0..n) of the plan's product (n = 2, or the plan's factors for a chain).
+void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
     if (!p) throw Error(kEInval, "null plan");
-    if (!a || !b) throw Error(kEInval, "null host buffer");
+    for (int f = 0; f < n; ++f)
+        if (!x[f]) throw Error(kEInval, "null host buffer");
     ensure_host_path(p);
     const size_t bytes = p->limbs() * sizeof(uint32_t);
     // Each operand goes in equal chunks of at most kDmaChunk: every copy thread stages its part of
@@ -357,11 +386,19 @@ void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
     // upload (so a arrives first at full link rate), and a's residue stage runs while b uploads.
     const size_t nchunks = (bytes + kDmaChunk - 1) / kDmaChunk;
     const size_t chunk = ((bytes + nchunks - 1) / nchunks + 4095) / 4096 * 4096;
-    const char* srcs[2] = {reinterpret_cast<const char*>(a), reinterpret_cast<const char*>(b)};
-    char* pins[2] = {reinterpret_cast<char*>(p->h_a), reinterpret_cast<char*>(p->h_b)};
-    char* devs[2] = {reinterpret_cast<char*>(p->d_a), reinterpret_cast<char*>(p->d_b)};
-    cudaStream_t streams[2] = {p->stream, p->copy_stream};
-    for (int op = 0; op < 2; ++op) {
+    const char* srcs[kMaxFactors];
+    char* pins[kMaxFactors];
+    char* devs[kMaxFactors];
+    uint32_t* dev_ops[kMaxFactors];
+    for (int f = 0; f < n; ++f) {
+        srcs[f] = reinterpret_cast<const char*>(x[f]);
+        uint32_t* pin = f == 0 ? p->h_a : f == 1 ? p->h_b : p->h_x[f - 2];
+        dev_ops[f] = f == 0 ? p->d_a : f == 1 ? p->d_b : p->d_x[f - 2];
+        pins[f] = reinterpret_cast<char*>(pin);
+        devs[f] = reinterpret_cast<char*>(dev_ops[f]);
+    }
+    for (int op = 0; op < n; ++op) {
+        cudaStream_t stream = op == 0 ? p->stream : p->copy_stream;
         if (op == 1) {
             // b's buffers may still be read by the plan's stream (a previous product): order the
             // copy stream after everything enqueued there so far, including a's upload
@@ -369,20 +406,20 @@ void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
             check(cudaStreamWaitEvent(p->copy_stream, p->ev_a, 0), "stream wait");
         }
         for (size_t off = 0; off < bytes; off += chunk) {
-            const size_t n = std::min(chunk, bytes - off);
+            const size_t len = std::min(chunk, bytes - off);
             p->pool->run([&](int part, int parts) {
                 size_t lo, hi;
-                slice(n, part, parts, &lo, &hi);
+                slice(len, part, parts, &lo, &hi);
                 if (hi > lo) std::memcpy(pins[op] + off + lo, srcs[op] + off + lo, hi - lo);
             });
-            check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, n, cudaMemcpyHostToDevice, streams[op]),
+            check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, len, cudaMemcpyHostToDevice, stream),
                   "operand copy");
         }
     }
     check(cudaEventRecord(p->ev_b, p->copy_stream), "event");
     check(cudaEventRecord(p->ev_start, p->stream), "event");
-    check(launch_product(p->desc(p->d_a, p->d_b, p->d_c), p->tables->view(), p->cfg, p->stream,
-                         p->timing ? p->ev_stage : nullptr, p->ev_b),
+    const ProductDesc d = n == 2 ? p->desc(p->d_a, p->d_b, p->d_c) : p->desc_chain(dev_ops, p->d_c);
+    check(launch_product(d, p->tables->view(), p->cfg, p->stream, p->timing ? p->ev_stage : nullptr, p->ev_b),
           "kernel launch");
     check(cudaEventRecord(p->ev_stop, p->stream), "event");
     size_t out_chunk;
@@ -394,6 +431,13 @@ void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
               "product copy");
         check(cudaEventRecord(p->ev_out[size_t(j)], p->stream), "event");
     }
+}
+
+}  // namespace
+
+void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b) {
+    const uint32_t* x[2] = {a, b};
+    submit_host_operands(p, x, 2);
 }
 
 void plan_collect_host(Plan* p, uint32_t* c) {
@@ -430,6 +474,28 @@ void plan_collect_host(Plan* p, uint32_t* c) {
 void plan_multiply_host(Plan* p, const uint32_t* a, const uint32_t* b, uint32_t* c) {
     plan_submit_host(p, a, b);
     plan_collect_host(p, c);
+}
+
+void plan_multiply_chain_host(Plan* p, const uint32_t* const* x, uint32_t* c) {
+    if (!p) throw Error(kEInval, "null plan");
+    if (!x) throw Error(kEInval, "null operand list");
+    submit_host_operands(p, x, p->factors);
+    plan_collect_host(p, c);
+}
+
+void plan_multiply_chain_device(Plan* p, const uint32_t* const* d_x, uint32_t* d_c, cudaStream_t stream) {
+    if (!p) throw Error(kEInval, "null plan");
+    if (!d_x || !d_c) throw Error(kEInval, "null device buffer");
+    uintptr_t align = reinterpret_cast<uintptr_t>(d_c);
+    for (int f = 0; f < p->factors; ++f) {
+        if (!d_x[f]) throw Error(kEInval, "null device buffer");
+        align |= reinterpret_cast<uintptr_t>(d_x[f]);
+    }
+    if (align & 15) throw Error(kEInval, "device buffers must be 16-byte aligned");
+    ensure_scratch(p);
+    check(launch_product(p->desc_chain(d_x, d_c), p->tables->view(), p->cfg, stream,
+                         p->timing ? p->ev_stage : nullptr),
+          "kernel launch");
 }
 
 // ------------------------------------------------------------------------------ row configuration

@@ -73,6 +73,10 @@ struct Plan {
     QConst* d_qc = nullptr;
     uint64_t* d_ra = nullptr;
     uint64_t* d_rb = nullptr;
+    int factors = 2;                                    // operands the plan's primes cover
+    uint64_t* d_rx[kMaxFactors - 2] = {};               // residues of operands 3, 4 (chained plans)
+    uint32_t* d_x[kMaxFactors - 2] = {};                // host path: device copies of operands 3, 4
+    uint32_t* h_x[kMaxFactors - 2] = {};                // host path: pinned staging of operands 3, 4
     uint32_t* d_a = nullptr;
     uint32_t* d_b = nullptr;
     uint32_t* d_c = nullptr;
@@ -95,10 +99,13 @@ struct Plan {
 
     size_t limbs() const { return size_t(N) * size_t(L); }
     ProductDesc desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const;
+    // All `factors` operands of a chained product (device pointers).
+    ProductDesc desc_chain(const uint32_t* const* x, uint32_t* c) const;
 };
 
-// W is the bit width the platform states for q; 0 means "take it from q".
-Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q);
+// W is the bit width the platform states for q; 0 means "take it from q". `factors` (2 to 4) is
+// the number of operands one product multiplies: the prime count covers the bound of that many.
+Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int factors = 2);
 void plan_destroy(Plan* p);
 
 // Plain-path resources, allocated on first use (cheap plans for batches and servers).
@@ -107,6 +114,9 @@ void ensure_host_path(Plan* p);
 
 // Device-resident product on `stream` (0: the CUDA default stream). Asynchronous.
 void plan_multiply_device(Plan* p, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t stream);
+// Chained product of the plan's `factors` device operands x[0..factors): one residue stage per
+// operand, every forward transform and pointwise product, one inverse transform, one CRT.
+void plan_multiply_chain_device(Plan* p, const uint32_t* const* d_x, uint32_t* d_c, cudaStream_t stream);
 
 // Host buffers in and out (the fherma_run contract), in two halves so a caller can do host work
 // while the GPU computes. submit: every pool thread stages a slice of a and b into pinned memory
@@ -115,6 +125,8 @@ void plan_multiply_device(Plan* p, const uint32_t* d_a, const uint32_t* d_b, uin
 void plan_submit_host(Plan* p, const uint32_t* a, const uint32_t* b);
 void plan_collect_host(Plan* p, uint32_t* c);
 void plan_multiply_host(Plan* p, const uint32_t* a, const uint32_t* b, uint32_t* c);
+// The chained product with host operands x[0..factors) (same staging as the pair).
+void plan_multiply_chain_host(Plan* p, const uint32_t* const* x, uint32_t* c);
 
 int current_device();
 

@@ -190,8 +190,8 @@ const std::vector<PrimeConst>& prime_set() {
     return set;
 }
 
-int primes_needed(int logN, int qbits) {
-    const int bound_bits = logN + 2 * qbits + 4;
+int primes_needed(int logN, int qbits, int factors) {
+    const int bound_bits = (factors - 1) * logN + factors * qbits + 4;
     Big prod{1};
     const auto& ps = prime_set();
     for (int k = 1; k <= kMaxPrimes; ++k) {
@@ -254,13 +254,14 @@ const HostTables& host_tables() {
     return t;
 }
 
-std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out) {
+std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out, int factors) {
     if (L < 1 || L > kMaxL) return "L must be between 1 and 32";
     if (logN < 1 || logN > kMaxLogN) return "N must be a power of two from 2 to 65536";
     if ((q[0] & 1u) == 0) return "q must be odd";
     const int qbits = bit_length(q, L);
     if (qbits <= 32 * (L - 1)) return "the top limb of q must be nonzero";
-    const int k = primes_needed(logN, qbits);
+    if (factors < 2 || factors > kMaxFactors) return "a product has 2 to 4 factors";
+    const int k = primes_needed(logN, qbits, factors);
     if (k < 0) return "the coefficient bound does not fit the 48-prime residue budget";
     const auto& ps = prime_set();
 

@@ -30,10 +30,12 @@ int bit_length(const uint32_t* v, int L);
 
 // Number of primes of the set needed for ring degree 2^logN and a qbits-bit modulus, by the
 // reference's bound bitlen(prod p) >= logN + 2 qbits + 4 (solve.cu:1177-1204); -1 if > 48.
-int primes_needed(int logN, int qbits);
+// A product of `factors` operands has coefficients below N^(factors-1) q^factors, so its bound is
+// (factors - 1) logN + factors qbits + 4 (the reference's bound for factors = 2).
+int primes_needed(int logN, int qbits, int factors = 2);
 
 // Fill the CRT + Barrett constants. Returns an empty string or an error message.
-std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out);
+std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out, int factors = 2);
 
 // Small helpers shared with the tests of the host math.
 uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t p);

@@ -66,17 +66,19 @@ cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfi
     Tables tt = t;
     cudaError_t e;
     if (ev && (e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
+    const int factors = d.mode == kModeProduct ? int(d.factors) : 1;
     if (b_ready && d.mode == kModeProduct) {
+        // operand a, then (once the others have landed) every other operand
         int tiles = g.tiles;
         for (int first = 0; first < 2; ++first) {
             if (first == 1 && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
             void* args[] = {&dd, &tt, &first, &tiles};
-            e = launch(dec, g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);
+            e = launch(dec, (first == 0 ? 1 : factors - 1) * g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);
             if (e != cudaSuccess) return e;
         }
     } else {
         int first = d.mode == kModeCachedA ? 1 : 0;
-        int count = d.mode == kModeProduct ? 2 : 1;
+        int count = factors;
         int tiles = g.tiles;
         void* args[] = {&dd, &tt, &first, &tiles};
         e = launch(dec, count * g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);

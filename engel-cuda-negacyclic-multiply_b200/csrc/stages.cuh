@@ -183,8 +183,8 @@ __device__ void dec_tile(const ProductDesc& d, const Tables& t, int operand, int
     const int T = N < kTile ? N : kTile;
     const int C = T >> logN1;
     const int L = int(d.L), k = int(d.k);
-    const uint32_t* x = operand ? d.b : d.a;
-    uint64_t* R = operand ? d.rb : d.ra;
+    const uint32_t* x = factor_limbs(d, operand);
+    uint64_t* R = factor_residues(d, operand);
     uint32_t* s_in = reinterpret_cast<uint32_t*>(smem);
     uint64_t* s_res = reinterpret_cast<uint64_t*>(smem);
     uint64_t* s_pow = reinterpret_cast<uint64_t*>(smem + dec_main_bytes(k));
@@ -381,11 +381,16 @@ __device__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint
         }
         row_store<S, LAST>(v, buf_a, lt);
     }
+    // factors 1 .. factors-1: forward transform, then pointwise product with the running product
+    // in buf_a (each thread reads and writes only its own positions there)
+    const int nf = d.mode == kModeProduct ? int(d.factors) : 2;
+    for (int f = 1; f < nf; ++f) {
+        if (f > 1) row_store<S, LAST>(v, buf_a, lt);
+        const uint64_t* R = factor_residues(d, f);
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(d.rb + off + row_index<S, 0>(lt, e)) : 0;
-    row_forward_from<S, 0>(v, buf, twf, base, lt, p);
-    __syncthreads();
-    {
+        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(R + off + row_index<S, 0>(lt, e)) : 0;
+        row_forward_from<S, 0>(v, buf, twf, base, lt, p);
+        __syncthreads();
         const uint64_t p2 = 2 * p;
         if (S::lolog(LAST) == 0 && S::r(LAST) >= 1) {
 #pragma unroll

@@ -34,6 +34,11 @@ C_SYMBOLS = [
     ("nc_multiply", ctypes.c_int, [_vp, _u32p, _u32p, _u32p]),
     ("nc_multiply_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
     ("nc_multiply_device_noalloc", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    ("nc_plan_create_chain", ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.c_int,
+                                            ctypes.POINTER(_vp)]),
+    ("nc_plan_factors", ctypes.c_int, [_vp]),
+    ("nc_multiply_chain", ctypes.c_int, [_vp, ctypes.POINTER(_u32p), _u32p]),
+    ("nc_multiply_chain_device", ctypes.c_int, [_vp, ctypes.POINTER(_vp), _vp, _vp]),
     ("nc_plan_set_crt_engine", ctypes.c_int, [_vp, ctypes.c_int]),
     ("nc_plan_get_crt_engine", ctypes.c_int, [_vp]),
     ("nc_plan_synchronize", ctypes.c_int, [_vp]),
@@ -137,11 +142,17 @@ def residues_gave_up() -> bool:
 class Plan:
     """One (N, q) configuration on the current CUDA device."""
 
-    def __init__(self, N: int, q_limbs: np.ndarray, W: int = 0):
+    def __init__(self, N: int, q_limbs: np.ndarray, W: int = 0, factors: int = 2):
+        """factors > 2 makes a chain plan: its primes cover products of that many operands
+        (multiply_chain); it still runs ordinary two-operand products."""
         q = np.ascontiguousarray(q_limbs, dtype=np.uint32)
         self.N, self.L = int(N), int(q.size)
         self._h = _vp()
-        _check(load().nc_plan_create(self.N, int(W), self.L, _u32(q), ctypes.byref(self._h)))
+        if factors == 2:
+            _check(load().nc_plan_create(self.N, int(W), self.L, _u32(q), ctypes.byref(self._h)))
+        else:
+            _check(load().nc_plan_create_chain(self.N, int(W), self.L, _u32(q), int(factors), ctypes.byref(self._h)))
+        self.factors = int(load().nc_plan_factors(self._h))
         n, l, k, qb = (ctypes.c_uint32() for _ in range(4))
         _check(load().nc_plan_query(self._h, ctypes.byref(n), ctypes.byref(l), ctypes.byref(k), ctypes.byref(qb)))
         self.k, self.qbits = int(k.value), int(qb.value)
@@ -163,6 +174,25 @@ class Plan:
     def multiply_device(self, d_a: int, d_b: int, d_c: int, stream: int = 0) -> None:
         """Device pointers (e.g. torch tensor .data_ptr()), enqueued on `stream` (0: default stream)."""
         _check(load().nc_multiply_device(self._h, _vp(d_a), _vp(d_b), _vp(d_c), _vp(stream or None)))
+
+    def multiply_chain(self, xs, out: np.ndarray | None = None) -> np.ndarray:
+        """Product of the plan's `factors` host operands (N, L) u32 (nc_multiply_chain)."""
+        if len(xs) != self.factors:
+            raise NegacyclicError(NC_EINVAL, f"the plan multiplies {self.factors} operands")
+        xs = [np.ascontiguousarray(x, dtype=np.uint32) for x in xs]
+        if any(x.size != self.N * self.L for x in xs):
+            raise NegacyclicError(NC_EINVAL, "every operand must contain N*L limbs")
+        ptrs = (_u32p * len(xs))(*[_u32(x) for x in xs])
+        c = out if out is not None else np.empty((self.N, self.L), dtype=np.uint32)
+        _check(load().nc_multiply_chain(self._h, ptrs, _u32(c)))
+        return c
+
+    def multiply_chain_device(self, d_xs, d_c: int, stream: int = 0) -> None:
+        """Device pointers of the plan's `factors` operands, enqueued on `stream`."""
+        if len(d_xs) != self.factors:
+            raise NegacyclicError(NC_EINVAL, f"the plan multiplies {self.factors} operands")
+        ptrs = (_vp * len(d_xs))(*[_vp(int(x)) for x in d_xs])
+        _check(load().nc_multiply_chain_device(self._h, ptrs, _vp(d_c), _vp(stream or None)))
 
     def multiply_device_noalloc(self, d_a: int, d_b: int, d_c: int, stream: int = 0) -> None:
         """Like multiply_device, but allocates nothing: for callers that must not allocate device

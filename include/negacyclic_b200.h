@@ -68,6 +68,23 @@ int nc_multiply_device(nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, 
 int nc_multiply_device_noalloc(const nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
                                void* stream);
 
+/* Chained product c = x_0 * x_1 * ... * x_{m-1} mod (X^N + 1, q) of m = 2..4 operands in one
+   pass: one residue stage per operand, every forward transform and pointwise product in the row
+   stage, then a single inverse transform and a single CRT. The plan's primes cover the bound of
+   m canonical operands, (m - 1) log2 N + m bits(q) + 4 bits, within the same 48 primes: at
+   N = 65536, m = 3 takes an 868-bit q (43 primes) and m = 4 a q of up to 731 bits; a larger q
+   returns NC_EINVAL. The output
+   equals the reference's pairwise products chained on the host (fherma_run twice or three times,
+   solve.cu:1489-1528), with one CRT and one copy-out instead of m - 1. Such a plan also runs
+   ordinary two-operand products (nc_multiply, batches, servers) with its larger prime set.
+   nc_plan_factors returns m (2 for nc_plan_create). x points to m operand pointers. */
+int nc_plan_create_chain(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int factors, nc_plan** out);
+int nc_plan_factors(const nc_plan* plan);
+/* Host operands, synchronous (the nc_multiply contract). */
+int nc_multiply_chain(nc_plan* plan, const uint32_t* const* x, uint32_t* c);
+/* Device operands (16-byte aligned), enqueued on `stream` (the nc_multiply_device contract). */
+int nc_multiply_chain_device(nc_plan* plan, const uint32_t* const* d_x, uint32_t* d_c, void* stream);
+
 /* Engine of the CRT accumulation sum_i v_i (M/p_i mod q) on the plan's plain path (the counterpart
    of fast_crt_kernel's 34-limb multiply-adds, solve.cu:752-836):
      NC_CRT_TC_I8  the default when the plan has at most 32 primes (q up to about 960 bits): an exact

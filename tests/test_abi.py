@@ -121,3 +121,29 @@ def test_batch_entry_points_reject_nulls():
     assert lib.nc_batch_run(None, None, 1) == nc.NC_EINVAL
     assert lib.nc_batch_destroy(None) == nc.NC_OK
     assert lib.nc_plan_hat_words(None) == 0
+
+
+@pytest.mark.parametrize("factors,bits,msg", [(1, 64, "factors must"), (5, 64, "factors must"),
+                                              (4, 868, "48-prime"), (4, 732, "48-prime")])
+def test_chain_plans_rejected_before_any_device_work(factors, bits, msg):
+    """A chain plan whose operand count is outside 2..4, or whose coefficient bound
+    (m - 1) log2 N + m bits(q) + 4 exceeds the 48 primes (m = 4 at N = 65536 allows 731 bits)."""
+    import ctypes
+
+    import cases
+
+    L = (bits + 31) // 32
+    q = cases.limbs_of(cases.gen_prime(bits, 95), L)
+    h = ctypes.c_void_p()
+    st = nc.load().nc_plan_create_chain(65536, 0, L, nc._u32(q), factors, ctypes.byref(h))
+    assert st == nc.NC_EINVAL
+    assert msg in nc.load().nc_last_error().decode()
+    assert not h.value
+
+
+def test_chain_entry_points_reject_nulls():
+    lib = nc.load()
+    assert lib.nc_plan_create_chain(8, 0, 1, None, 3, None) == nc.NC_EINVAL
+    assert lib.nc_multiply_chain(None, None, None) == nc.NC_EINVAL
+    assert lib.nc_multiply_chain_device(None, None, None, None) == nc.NC_EINVAL
+    assert lib.nc_plan_factors(None) == nc.NC_EINVAL
