@@ -407,6 +407,7 @@ def ours(args) -> dict | None:
                               ("batched_c3", "batched 64 x N=16384", lambda: batched_same_shape(dev, case.q, 16384, 64, args)),
                               ("uneven_c4", "uneven batch", lambda: uneven_batch(dev, mix, args)),
                               ("ablation_residues", "residue ablation", lambda: residue_ablation(dev, case)),
+                              ("chained_n65536", "chained products", lambda: chained(dev)),
                               ("serve_c5", "serving", lambda: serving(dev, mix, args))):
             log(what)
             try:
@@ -488,6 +489,74 @@ def residue_ablation(dev, case, reps: int = 20) -> dict:
             "tc_i8_int8_tops": 2 * 2 * 128 * (8 * ((k + 1) & ~1)) * N / (ms["tc_i8"] * 1e-3) / 1e12,
             "imad_limb_macs_per_s": macs / (ms["imad"] * 1e-3), "hbm_bytes": hbm_bytes,
             "l2": "flushed (256 MiB write) before each timed pair"}
+
+
+def _flushed_ms(fn, flush, reps: int) -> float:
+    """Median CUDA-event milliseconds of fn() over `reps` runs, L2 flushed before each."""
+    import torch
+
+    for _ in range(3):
+        fn()
+    times = []
+    for _ in range(reps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return statistics.median(times)
+
+
+def chained(dev, reps: int = 10) -> dict:
+    """x_0 x_1 ... x_{m-1} at N=65536 as one chained product (one residue stage per operand, one
+    row launch with every forward transform and pointwise product, one inverse transform and CRT)
+    against m - 1 plain products where each feeds the next, device-resident, L2 flushed before each
+    timed run; both outputs compared."""
+    import numpy as np
+    import torch
+
+    import cases
+    import negacyclic as nc
+
+    N = 65536
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    out = {}
+    for m, bits in ((3, 868), (4, 731), (4, 434)):
+        L = (bits + 31) // 32
+        q = cases.gen_prime(bits, 4000 + bits)
+        ql = cases.limbs_of(q, L)
+        xs = [torch.from_numpy(cases.coeffs(q, N, L, 4100 + f).view(np.int32)).to(dev) for f in range(m)]
+        c_chain, c_pair, tmp = (torch.empty_like(xs[0]) for _ in range(3))
+        with nc.Plan(N, ql, factors=m) as chain, nc.Plan(N, ql) as pair:
+            chain.autotune(reps=2)
+            pair.autotune(reps=2)
+            ptrs = [x.data_ptr() for x in xs]
+
+            def run_chain():
+                chain.multiply_chain_device(ptrs, c_chain.data_ptr(), 0)
+
+            # ping-pong so that the last product lands in c_pair
+            bufs = [c_pair.data_ptr() if (m - 2 - i) % 2 == 0 else tmp.data_ptr() for i in range(m - 1)]
+
+            def run_pairs():
+                pair.multiply_device(ptrs[0], ptrs[1], bufs[0], 0)
+                for i, x in enumerate(ptrs[2:], start=1):
+                    pair.multiply_device(bufs[i - 1], x, bufs[i], 0)
+
+            ms_chain = _flushed_ms(run_chain, flush, reps)
+            ms_pairs = _flushed_ms(run_pairs, flush, reps)
+            exact = bool(torch.equal(c_chain, c_pair))
+            k_chain, k_pair = chain.k, pair.k
+        if not exact:
+            raise RuntimeError(f"chained and pairwise products differ (m={m}, {bits}-bit q)")
+        out[f"m{m}_q{bits}"] = {"chain_us": 1e3 * ms_chain, "pairwise_us": 1e3 * ms_pairs,
+                                "speedup": ms_pairs / ms_chain, "primes_chain": k_chain,
+                                "primes_pairwise": k_pair, "bit_exact_vs_pairwise": exact}
+    out["form"] = ("N=65536, device-resident; pairwise = m - 1 plain products, each output the next "
+                   "product's operand; L2 flushed before each timed run; median of 10")
+    return out
 
 
 def batched_same_shape(dev, q: int, N: int, count: int, args) -> dict:

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <map>
 
+#include "hostcopy.h"
 #include "hostmath.h"
 #include "kernels.h"
 
@@ -287,6 +288,7 @@ void ensure_host_path(Plan* p) {
     check(cudaMallocHost(&p->h_a, limbs), "pinned a");
     check(cudaMallocHost(&p->h_b, limbs), "pinned b");
     check(cudaMallocHost(&p->h_c, limbs), "pinned c");
+    check(cudaMalloc(&p->d_hat, size_t(p->k) * p->N * sizeof(uint64_t)), "operand a in the NTT domain");
     for (int f = 2; f < p->factors; ++f) {
         check(cudaMalloc(&p->d_x[f - 2], limbs), "input operand");
         check(cudaMallocHost(&p->h_x[f - 2], limbs), "pinned operand");
@@ -312,6 +314,7 @@ void plan_destroy(Plan* p) {
     cudaFree(p->d_crt_b);
     cudaFree(p->d_ra);
     cudaFree(p->d_rb);
+    cudaFree(p->d_hat);
     for (int f = 0; f < kMaxFactors - 2; ++f) {
         cudaFree(p->d_rx[f]);
         cudaFree(p->d_x[f]);
@@ -397,12 +400,33 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
         pins[f] = reinterpret_cast<char*>(pin);
         devs[f] = reinterpret_cast<char*>(dev_ops[f]);
     }
+    ProductDesc d = n == 2 ? p->desc(p->d_a, p->d_b, p->d_c) : p->desc_chain(dev_ops, p->d_c);
     for (int op = 0; op < n; ++op) {
         cudaStream_t stream = op == 0 ? p->stream : p->copy_stream;
         if (op == 1) {
             // b's buffers may still be read by the plan's stream (a previous product): order the
             // copy stream after everything enqueued there so far, including a's upload
             check(cudaEventRecord(p->ev_a, p->stream), "event");
+            // a's stages go on the plan's stream now, before any copy of the other operands is
+            // queued: work queued on that stream behind a's upload after those copies were queued
+            // waited for them (measured: the kernel started only once b had landed). For a pair,
+            // that is a's residues and forward transforms (the GPU is otherwise idle while b
+            // uploads), and the product then takes a in the NTT domain; for a chain, a's residues.
+            check(cudaEventRecord(p->ev_start, p->stream), "event");
+            if (p->timing) check(cudaEventRecord(p->ev_stage[0], p->stream), "event");
+            if (n == 2) {
+                ProductDesc fa = d;
+                fa.mode = kModeForward;
+                fa.b = nullptr;
+                fa.c = nullptr;
+                fa.hat_out = p->d_hat;
+                check(launch_product(fa, p->tables->view(), p->cfg, p->stream), "kernel launch");
+                d.mode = kModeCachedA;
+                d.a = nullptr;
+                d.a_hat = p->d_hat;
+            } else {
+                check(launch_residues(d, p->tables->view(), p->cfg, p->stream, 0, 1), "kernel launch");
+            }
             check(cudaStreamWaitEvent(p->copy_stream, p->ev_a, 0), "stream wait");
         }
         for (size_t off = 0; off < bytes; off += chunk) {
@@ -410,15 +434,13 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
             p->pool->run([&](int part, int parts) {
                 size_t lo, hi;
                 slice(len, part, parts, &lo, &hi);
-                if (hi > lo) std::memcpy(pins[op] + off + lo, srcs[op] + off + lo, hi - lo);
+                if (hi > lo) stage_copy(pins[op] + off + lo, srcs[op] + off + lo, hi - lo);
             });
             check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, len, cudaMemcpyHostToDevice, stream),
                   "operand copy");
         }
     }
     check(cudaEventRecord(p->ev_b, p->copy_stream), "event");
-    check(cudaEventRecord(p->ev_start, p->stream), "event");
-    const ProductDesc d = n == 2 ? p->desc(p->d_a, p->d_b, p->d_c) : p->desc_chain(dev_ops, p->d_c);
     check(launch_product(d, p->tables->view(), p->cfg, p->stream, p->timing ? p->ev_stage : nullptr, p->ev_b),
           "kernel launch");
     check(cudaEventRecord(p->ev_stop, p->stream), "event");
@@ -462,8 +484,8 @@ void plan_collect_host(Plan* p, uint32_t* c) {
             size_t lo, hi;
             slice(n, part, parts, &lo, &hi);
             if (hi > lo)
-                std::memcpy(reinterpret_cast<char*>(c) + base + lo, reinterpret_cast<const char*>(p->h_c) + base + lo,
-                            hi - lo);
+                stage_copy(reinterpret_cast<char*>(c) + base + lo, reinterpret_cast<const char*>(p->h_c) + base + lo,
+                           hi - lo);
         }
     });
     check(cudaError_t(err.load()), "product");

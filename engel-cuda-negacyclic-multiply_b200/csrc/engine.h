@@ -83,6 +83,7 @@ struct Plan {
     uint32_t* h_a = nullptr;
     uint32_t* h_b = nullptr;
     uint32_t* h_c = nullptr;
+    uint64_t* d_hat = nullptr;  // host path: NTT form of operand a (k x N), made while b uploads
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     std::vector<cudaEvent_t> ev_out;  // one per output chunk (one chunk per pool part)

@@ -54,35 +54,39 @@ cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32) {
     return e;
 }
 
+cudaError_t launch_residues(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s, int first,
+                            int count) {
+    void* dec = dec_kernel(int(d.LW));
+    if (!dec) return cudaErrorInvalidValue;
+    const Geometry g = geometry(int(d.logN), int(d.k), cfg);
+    ProductDesc dd = d;
+    Tables tt = t;
+    int tiles = g.tiles;
+    void* args[] = {&dd, &tt, &first, &tiles};
+    return launch(dec, count * g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);
+}
+
 cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s,
                            cudaEvent_t* ev, cudaEvent_t b_ready) {
     if (int(d.logN2) != cfg.logN2) return cudaErrorInvalidValue;
     void* row = row_kernel(cfg);
-    void* dec = dec_kernel(int(d.LW));
     void* crt = d.crt_b ? crt_tc_kernel(int(d.LW)) : crt_kernel(int(d.LW));
-    if (!row || !dec || !crt) return cudaErrorInvalidValue;
+    if (!row || !crt || !dec_kernel(int(d.LW))) return cudaErrorInvalidValue;
     const Geometry g = geometry(int(d.logN), int(d.k), cfg);
     ProductDesc dd = d;
     Tables tt = t;
     cudaError_t e;
-    if (ev && (e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
     const int factors = d.mode == kModeProduct ? int(d.factors) : 1;
-    if (b_ready && d.mode == kModeProduct) {
-        // operand a, then (once the others have landed) every other operand
-        int tiles = g.tiles;
-        for (int first = 0; first < 2; ++first) {
-            if (first == 1 && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
-            void* args[] = {&dd, &tt, &first, &tiles};
-            e = launch(dec, (first == 0 ? 1 : factors - 1) * g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);
-            if (e != cudaSuccess) return e;
-        }
+    if (b_ready && d.mode != kModeForward) {
+        // operand a is already taken care of on s (its residues, or its NTT form for a cached-a
+        // product); the other operands follow once they have landed
+        if ((e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
+        const int rest = d.mode == kModeProduct ? factors - 1 : 1;
+        if ((e = launch_residues(d, t, cfg, s, 1, rest)) != cudaSuccess) return e;
     } else {
-        int first = d.mode == kModeCachedA ? 1 : 0;
-        int count = factors;
-        int tiles = g.tiles;
-        void* args[] = {&dd, &tt, &first, &tiles};
-        e = launch(dec, count * g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);
-        if (e != cudaSuccess) return e;
+        if (ev && (e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
+        const int first = d.mode == kModeCachedA ? 1 : 0;
+        if ((e = launch_residues(d, t, cfg, s, first, factors)) != cudaSuccess) return e;
     }
     if (ev && (e = cudaEventRecord(ev[1], s)) != cudaSuccess) return e;
     {

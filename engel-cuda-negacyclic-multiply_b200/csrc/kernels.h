@@ -19,11 +19,18 @@ cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32);
 std::vector<RowConfig> row_variants(int logN);
 bool row_variant_exists(const RowConfig& c);
 
+// Enqueue the residue stage (with the forward column stages) of operands [first, first + count)
+// of the product on stream s.
+cudaError_t launch_residues(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s, int first,
+                            int count);
+
 // Enqueue the three stages of one product on stream s. With `stage_events` (4 events), event i
-// is recorded before stage i and event 3 after the last stage. With `b_ready` (product mode
-// only), the residue stage of operand a is enqueued first and s then waits for b_ready before the
-// residue stage of operand b, so a's residues overlap b's upload on another stream; b_ready
-// must already be recorded.
+// is recorded before stage i and event 3 after the last stage. With `b_ready` (product and
+// cached-a modes), operand a must already be taken care of on s (product: its residue stage,
+// launch_residues(d, .., 0, 1); cached-a: a forward-mode launch that wrote d.a_hat), with stage
+// event 0 recorded before that by the caller: s waits for b_ready, then runs the residue stage
+// of the other operands, so a's stages overlap their upload on another stream. b_ready must
+// already be recorded.
 cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s,
                            cudaEvent_t* stage_events = nullptr, cudaEvent_t b_ready = nullptr);
 

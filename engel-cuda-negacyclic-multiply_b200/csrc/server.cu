@@ -1,6 +1,8 @@
 // Serving loop (see server.h).
 #include "server.h"
 
+#include "hostcopy.h"
+
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -199,8 +201,8 @@ uint64_t Server::submit(Plan* plan, const uint32_t* a, int operand, const uint32
         r->id = next_id_++;
     }
     const size_t bytes = plan->limbs() * 4;
-    if (operand < 0) std::memcpy(r->host, a, bytes);
-    std::memcpy(r->host + r->limb_bytes, b, bytes);
+    if (operand < 0) stage_copy(r->host, reinterpret_cast<const char*>(a), bytes);
+    stage_copy(r->host + r->limb_bytes, reinterpret_cast<const char*>(b), bytes);
     std::lock_guard<std::mutex> lock(mu_);
     r->t_submit = now_ms();
     if (t_first_ < 0) t_first_ = r->t_submit;
