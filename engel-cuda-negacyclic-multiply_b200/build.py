@@ -30,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", f"-I{INCLUDE}", f"-I{CSRC}"]
 
 LIB_SOURCES = ["hostmath.cpp", "k_dec.cu", "k_row.cu", "k_crt.cu", "k_batch.cu", "kernels.cu", "batch.cu",
-               "engine.cu", "server.cu", "api.cu", "noalloc.cu", "k_residues.cu", "k_crt_tc.cu"]
+               "engine.cu", "server.cu", "api.cu", "noalloc.cu", "k_residues.cu", "k_crt_tc.cu", "k_dec_tc.cu"]
 RUNNER_SOURCES = ["runner.cpp"]
 
 

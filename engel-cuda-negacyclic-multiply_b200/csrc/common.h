@@ -78,6 +78,7 @@ struct ProductDesc {
     uint32_t factors;       // operands of the product (2: a b; 3, 4: a b x_more[0] [x_more[1]])
     const uint32_t* x_more[kMaxFactors - 2];  // further operands (N x L limbs)
     uint64_t* r_more[kMaxFactors - 2];        // their residues (k x N scratch)
+    uint32_t res_tc;        // residue stage of the plain path on the tensor cores (k <= 32)
 };
 
 // Operand f of a product (0: a, 1: b, 2..: x_more) and its residue buffer.
@@ -98,6 +99,7 @@ struct Tables {
     const ulonglong2* inv;    // [kMaxPrimes][kMaxN]
     const uint64_t* pow32;    // [kMaxPrimes][kMaxL]: 2^(32 l) mod p_i
     const uint64_t* primes;   // [kMaxPrimes]
+    const uint4* res_w;       // [kMaxPrimes][8 K chunks][8 byte planes][16 B]: byte c of 2^(8 b) mod p_i
 };
 
 // Dynamic shared memory of each stage.
@@ -128,6 +130,18 @@ NC_HD constexpr size_t crt_tc_smem_bytes(int LW) {
     return smax(size_t(2) * kCrtTcHalfBytes + crt_tc_table_bytes(LW) + size_t(kCrtTcMaxPrimes) * 8 * 3 +
                     size_t(kMqStride) * 4 * 2 + 16 + 16,
                 (size_t(233472) / (512 / crt_tc_tmem_cols(LW) + 1) + 16) / 16 * 16);
+}
+
+// Residue stage on the tensor cores (plain path): a tile of 128 coefficients (the MMA's M) x 128
+// K bytes of limbs, the weight bytes of up to 32 primes, and p_i; the primes go through the MMA in
+// passes of 16 (128 accumulator columns), so tensor memory holds four CTAs per SM. The shared
+// memory is raised to keep it at four.
+constexpr int kDecTcRows = 128;
+constexpr int kDecTcPassPrimes = 16;
+constexpr uint32_t kDecTcCols = 128;
+NC_HD constexpr size_t dec_tc_smem_bytes(int k) {
+    return smax(size_t(kDecTcRows) * 128 + size_t((k + 1) & ~1) * 1024 + size_t(kCrtTcMaxPrimes) * 8,
+                (size_t(233472) / (512 / kDecTcCols + 1) + 16) / 16 * 16);
 }
 
 // How the row stage tiles a product: row blocks of N2 = 2^logN2 residues, each thread holding

@@ -60,6 +60,20 @@ DeviceTables* acquire_tables(int device) {
               "limb weight upload");
         check(cudaMemcpy(t->primes, primes.data(), size_t(kMaxPrimes) * sizeof(uint64_t), cudaMemcpyHostToDevice),
               "prime upload");
+        // weight bytes of the tensor-core residue stage: byte c of 2^(8 b) mod p_i at
+        // [i][b / 16][c][b % 16], b < 128 (the K bytes of up to 32 limbs)
+        std::vector<uint8_t> w(size_t(kMaxPrimes) * 1024, 0);
+        for (int i = 0; i < kMaxPrimes; ++i) {
+            const uint64_t p = h.pc[size_t(i)].p;
+            uint64_t v = 1;
+            for (int b = 0; b < 128; ++b) {
+                for (int c = 0; c < 8; ++c)
+                    w[size_t(i) * 1024 + size_t(b / 16) * 128 + size_t(c) * 16 + size_t(b % 16)] = uint8_t(v >> (8 * c));
+                v = uint64_t((unsigned __int128)v * 256u % p);
+            }
+        }
+        check(cudaMalloc(&t->res_w, w.size()), "residue weight table");
+        check(cudaMemcpy(t->res_w, w.data(), w.size(), cudaMemcpyHostToDevice), "residue weight upload");
         check(prepare_kernels(h.pc.data(), h.pow32.data()), "kernel preparation");
         // a synchronous copy from pageable memory may return before its last DMA lands, and the
         // kernels run on non-blocking streams that do not order after it: wait for the device
@@ -69,6 +83,7 @@ DeviceTables* acquire_tables(int device) {
         cudaFree(t->inv);
         cudaFree(t->pow32);
         cudaFree(t->primes);
+        cudaFree(t->res_w);
         delete t;
         throw;
     }
@@ -89,6 +104,7 @@ void release_tables(DeviceTables* t) {
     cudaFree(t->inv);
     cudaFree(t->pow32);
     cudaFree(t->primes);
+    cudaFree(t->res_w);
     cudaSetDevice(prev);
     delete t;
 }
@@ -163,6 +179,7 @@ ProductDesc Plan::desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const 
     d.logN2 = uint32_t(cfg.logN2);
     d.crt_b = crt_tc ? d_crt_b : nullptr;
     d.factors = 2;
+    d.res_tc = res_tc && k <= kCrtTcMaxPrimes ? 1u : 0u;
     return d;
 }
 

@@ -36,7 +36,8 @@ struct DeviceTables {
     ulonglong2* inv = nullptr;
     uint64_t* pow32 = nullptr;   // [kMaxPrimes][kMaxL]
     uint64_t* primes = nullptr;  // [kMaxPrimes]
-    Tables view() const { return Tables{fwd, inv, pow32, primes}; }
+    uint4* res_w = nullptr;      // weight bytes of the tensor-core residue stage
+    Tables view() const { return Tables{fwd, inv, pow32, primes, res_w}; }
 };
 
 DeviceTables* acquire_tables(int device);
@@ -95,6 +96,7 @@ struct Plan {
     RowConfig cfg{};                 // row-stage tiling of the plain path (autotuned per N)
     uint4* d_crt_b = nullptr;        // byte table of the tensor-core CRT (k <= 32), built at creation
     bool crt_tc = true;              // plain path: CRT accumulation on the tensor cores when available
+    bool res_tc = true;              // plain path: residue stage on the tensor cores when k <= 32
     bool timing = false;             // record per-stage events
     cudaEvent_t ev_stage[4] = {nullptr, nullptr, nullptr, nullptr};
 

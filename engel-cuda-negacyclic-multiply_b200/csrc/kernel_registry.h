@@ -12,12 +12,14 @@
 namespace nc {
 
 void* dec_kernel(int LW);
+void* dec_tc_kernel(int logN1);
 void* crt_kernel(int LW);
 void* crt_tc_kernel(int LW);
 void* row_kernel(const RowConfig& c);
 std::vector<RowConfig> all_row_variants();
 
 cudaError_t prepare_dec(const PrimeConst* pc, const uint64_t* pow32);
+cudaError_t prepare_dec_tc(const PrimeConst* pc, const uint64_t* pow32);
 cudaError_t prepare_crt(const PrimeConst* pc, const uint64_t* pow32);
 cudaError_t prepare_crt_tc(const PrimeConst* pc, const uint64_t* pow32);
 cudaError_t prepare_row(const PrimeConst* pc, const uint64_t* pow32);

@@ -46,6 +46,7 @@ std::vector<RowConfig> row_variants(int logN) {
 
 cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32) {
     cudaError_t e = prepare_dec(pc, pow32);
+    if (e == cudaSuccess) e = prepare_dec_tc(pc, pow32);
     if (e == cudaSuccess) e = prepare_row(pc, pow32);
     if (e == cudaSuccess) e = prepare_crt(pc, pow32);
     if (e == cudaSuccess) e = prepare_crt_tc(pc, pow32);
@@ -56,11 +57,20 @@ cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32) {
 
 cudaError_t launch_residues(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s, int first,
                             int count) {
+    ProductDesc dd = d;
+    Tables tt = t;
+    if (d.res_tc && int(d.k) <= kCrtTcMaxPrimes && t.res_w) {
+        // tensor-core residues: 128-coefficient tiles
+        void* dec = dec_tc_kernel(int(d.logN) - cfg.logN2);
+        if (!dec) return cudaErrorInvalidValue;
+        const int n = 1 << d.logN;
+        int tiles = n < kDecTcRows ? 1 : n / kDecTcRows;
+        void* args[] = {&dd, &tt, &first, &tiles};
+        return launch(dec, count * tiles, kThreads, dec_tc_smem_bytes(int(d.k)), s, args);
+    }
     void* dec = dec_kernel(int(d.LW));
     if (!dec) return cudaErrorInvalidValue;
     const Geometry g = geometry(int(d.logN), int(d.k), cfg);
-    ProductDesc dd = d;
-    Tables tt = t;
     int tiles = g.tiles;
     void* args[] = {&dd, &tt, &first, &tiles};
     return launch(dec, count * g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);

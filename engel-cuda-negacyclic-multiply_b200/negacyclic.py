@@ -50,6 +50,8 @@ C_SYMBOLS = [
     ("nc_primes", ctypes.c_int, [_u64p, ctypes.c_int]),
     ("nc_residues", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     ("nc_residues_status", ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    ("nc_plan_set_residue_engine", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nc_plan_get_residue_engine", ctypes.c_int, [_vp]),
     ("nc_row_variants", ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
     ("nc_plan_set_row_config", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nc_plan_get_row_config", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
@@ -216,6 +218,18 @@ class Plan:
     @crt_engine.setter
     def crt_engine(self, engine: int) -> None:
         _check(load().nc_plan_set_crt_engine(self._h, int(engine)))
+
+    @property
+    def residue_engine(self) -> int:
+        """RESIDUES_TC_I8 (default with at most 32 primes) or RESIDUES_IMAD for this plan's products."""
+        e = load().nc_plan_get_residue_engine(self._h)
+        if e < 0:
+            _check(e)
+        return e
+
+    @residue_engine.setter
+    def residue_engine(self, engine: int) -> None:
+        _check(load().nc_plan_set_residue_engine(self._h, int(engine)))
 
     def synchronize(self) -> None:
         _check(load().nc_plan_synchronize(self._h))

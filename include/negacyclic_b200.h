@@ -134,13 +134,24 @@ int nc_primes(uint64_t* out, int count);
  *                      2^(8 j) mod p_i (tcgen05.mma kind::i8, s32 accumulators in tensor memory),
  *                      recombined and reduced mod p_i; at most 32 primes (q up to about 960 bits).
  * The counterpart of both in the reference is to_residues_tiled_kernel (solve.cu:533-570), which
- * also multiplies by R^2 and psi^n. Not used by the product path: it exists to time the two engines
- * on the same input and check that they agree. d_x is 16-byte aligned; enqueued on `stream`. */
+ * also multiplies by R^2 and psi^n. This entry point runs the stage alone (no column stages), to
+ * time the two engines on the same input and check that they agree; the plan's own products pick
+ * theirs with nc_plan_set_residue_engine. d_x is 16-byte aligned; enqueued on `stream`. */
 enum { NC_RESIDUES_IMAD = 0, NC_RESIDUES_TC_I8 = 1 };
 int nc_residues(const nc_plan* plan, const uint32_t* d_x, uint64_t* d_r, int engine, void* stream);
 /* After the work has finished: 1 in *gave_up if a tensor-core launch on the current device gave up
    its bounded wait for the MMA (its residues are then not written); the flag is cleared. */
 int nc_residues_status(int* gave_up);
+
+/* Engine of the residue stage of the plan's own products (nc_multiply, nc_multiply_device, the
+   chained products; batches and servers keep the integer pipes inside their persistent launch):
+     NC_RESIDUES_TC_I8  the default when the plan has at most 32 primes: the contraction above on
+                        128-coefficient tiles, fused with the forward column stages (k_dec_tc);
+     NC_RESIDUES_IMAD   the integer-pipe residue stage (k_dec; always available).
+   Both give the same residues mod p_i and so the same product. Set it only while no product of
+   the plan is in flight; nc_plan_get_residue_engine returns the engine in use. */
+int nc_plan_set_residue_engine(nc_plan* plan, int engine);
+int nc_plan_get_residue_engine(const nc_plan* plan);
 
 /* ------------------------------------------------------------------ tuning */
 
