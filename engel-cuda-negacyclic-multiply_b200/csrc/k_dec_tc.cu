@@ -10,7 +10,7 @@
 // x 128 K bytes (4 L, zero padded) x 8 columns per prime, every S < 128 * 255^2 < 2^23, so the s32
 // accumulation in tensor memory is exact. The primes go through tcgen05.mma kind::i8 in passes of
 // 16 (128 accumulator columns); after each pass the eight warps read the partial sums back
-// (tcgen05.ld), fold sum_c 2^(8 c) S_c (< 2^80) and reduce it mod p_i into [0, 2p). The tile is
+// (tcgen05.ld) and fold sum_c 2^(8 c) S_c (< 2^80) into [0, 2p) modulo p_i. The tile is
 // C = 128 / N1 columns of all N1 rows of the polynomial (row length N2 = N / N1), as in k_dec, so
 // the forward column stages and the residue-row stores follow unchanged.
 //
@@ -41,20 +41,22 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src, uint32_t s
                  : "memory");
 }
 
-__device__ __forceinline__ void add128(uint64_t& lo, uint64_t& hi, uint64_t add_lo, uint64_t add_hi) {
-    const uint64_t s = lo + add_lo;
-    hi += add_hi + (s < lo ? 1u : 0u);
-    lo = s;
+// sum_c 2^(8 c) s[c] mod p = 2^62 - m, for s[c] < 2^23, into [0, 2p). With A = sum_{c<4} and
+// B = sum_{c>=4} 2^(8 (c - 4)) s[c] (both < 2^48) the value is A + B 2^32, and since
+// 2^62 = m (mod p), B 2^32 = (B >> 30) m + (B mod 2^30) 2^32, so the sum
+// A + (B mod 2^30) 2^32 + (B >> 30) m < 2^62 + 2^49 is below 2p: six wide multiply-adds, a
+// shift, a mask, one add and one more multiply-add.
+__device__ __forceinline__ uint64_t mad_wide(uint32_t a, uint32_t b, uint64_t c) {
+    uint64_t d;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"(b), "l"(c));
+    return d;
 }
-
-// sum_c 2^(8 c) s[c] (< 2^80) reduced mod p = 2^62 - m into [0, 2p).
-__device__ __forceinline__ uint64_t fold_planes(const uint32_t* s, uint64_t m) {
-    uint64_t lo = uint64_t(s[0]) + (uint64_t(s[1]) << 8) + (uint64_t(s[2]) << 16) + (uint64_t(s[3]) << 24) +
-                  (uint64_t(s[4]) << 32) + (uint64_t(s[5]) << 40);
-    uint64_t hi = 0;
-    add128(lo, hi, uint64_t(s[6]) << 48, uint64_t(s[6]) >> 16);
-    add128(lo, hi, uint64_t(s[7]) << 56, uint64_t(s[7]) >> 8);
-    return reduce_special(hi, lo, m);
+__device__ __forceinline__ uint64_t fold_planes(const uint32_t* s, uint32_t m) {
+    const uint64_t a = mad_wide(s[3], 1u << 24, mad_wide(s[2], 1u << 16, mad_wide(s[1], 1u << 8, uint64_t(s[0]))));
+    const uint64_t b = mad_wide(s[7], 1u << 24, mad_wide(s[6], 1u << 16, mad_wide(s[5], 1u << 8, uint64_t(s[4]))));
+    const uint32_t bq = uint32_t(b >> 30);                                      // < 2^18
+    const uint64_t r = a + (uint64_t(uint32_t(b) & ((1u << 30) - 1)) << 32);   // < 2^62 + 2^48
+    return mad_wide(bq, m, r);
 }
 
 // Residue row of prime i in shared memory (128 values): pass 0's primes over their own weights,
@@ -62,6 +64,10 @@ __device__ __forceinline__ uint64_t fold_planes(const uint32_t* s, uint64_t m) {
 __device__ __forceinline__ uint64_t* res_row(uint8_t* sA, uint8_t* sB, int i) {
     return reinterpret_cast<uint64_t*>(i < kDecTcPassPrimes ? sB + i * 1024 : sA + (i - kDecTcPassPrimes) * 1024);
 }
+
+// Slot of tile row x in prime i's residue row: rows XORed with (i C) mod 16, so that the 32 / C
+// primes one warp reads in the column stages (C consecutive rows each) fall on different banks.
+__device__ __forceinline__ int res_slot(int i, int x, int C) { return x ^ ((i * C) & 15); }
 
 // Four CTAs per SM where the column transform fits 64 registers; the 16- and 32-point columns
 // (N1 values per thread) take three and two.
@@ -177,8 +183,10 @@ __global__ void __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 
                       "=r"(s[15])
                     : "r"(lane_base + uint32_t(8 * (i - i0))));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                res_row(sA, sB, i)[m] = fold_planes(s, (uint64_t(1) << 62) - s_p[i]);
-                if (i + 1 < ie) res_row(sA, sB, i + 1)[m] = fold_planes(s + 8, (uint64_t(1) << 62) - s_p[i + 1]);
+                res_row(sA, sB, i)[res_slot(i, m, C)] = fold_planes(s, uint32_t((uint64_t(1) << 62) - s_p[i]));
+                if (i + 1 < ie)
+                    res_row(sA, sB, i + 1)[res_slot(i + 1, m, C)] =
+                        fold_planes(s + 8, uint32_t((uint64_t(1) << 62) - s_p[i + 1]));
             }
         } else if (m < T) {
             // the wait gave up: this warp's residues by the integer carry chains
@@ -190,7 +198,8 @@ __global__ void __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 
                     const uint64_t c = __ldg(t.pow32 + size_t(i) * kMaxL + l);
                     mac_u32x64(__ldg(row + l), uint32_t(c), uint32_t(c >> 32), a0, a1, a2, b0, b1, b2);
                 }
-                res_row(sA, sB, i)[m] = reduce_limb_sum(a0, a1, a2, b0, b1, b2, (uint64_t(1) << 62) - s_p[i]);
+                res_row(sA, sB, i)[res_slot(i, m, C)] =
+                    reduce_limb_sum(a0, a1, a2, b0, b1, b2, (uint64_t(1) << 62) - s_p[i]);
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -206,7 +215,7 @@ __global__ void __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 
         const uint64_t* sr = res_row(sA, sB, i);
         uint64_t v[N1];
 #pragma unroll
-        for (int u = 0; u < N1; ++u) v[u] = sr[u * C + j];
+        for (int u = 0; u < N1; ++u) v[u] = sr[res_slot(i, u * C + j, C)];
         if (LOG_N1 > 0) column_forward<LOG_N1>(t.fwd + size_t(i) * kMaxN, s_p[i], v);
         uint64_t* out = R + size_t(i) * N + j0 + j;
 #pragma unroll

@@ -2,8 +2,9 @@
 
     python profile_case.py --N 65536 --bits 868 --reps 3 [--config 12,3,512] [--batch 0]
 
-Each rep enqueues the three kernels of one product (k_dec, k_row, k_crt) on the default
-stream, with the given row configuration (default: the plan's default); with --batch B > 0
+Each rep enqueues the three kernels of one product (residues: k_dec_tc, or k_dec with
+--residue-engine imad; k_row; k_crt_tc) on the default stream, with the given row configuration
+(default: the plan's default); with --batch B > 0
 each rep is instead one persistent launch (k_persistent) of B products; with --residues
 imad|tc each rep is the residue stage alone of both operands (k_residues_imad or k_residues_tc).
 The run ends by checking the last result against the host entry point (or, for --residues,
@@ -26,6 +27,8 @@ def main() -> int:
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--config", type=str, default="")
     ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--residue-engine", choices=["tc", "imad"], default="tc",
+                    help="residue stage of the plan's products: k_dec_tc (tensor cores) or k_dec")
     ap.add_argument("--residues", choices=["", "imad", "tc"], default="",
                     help="run only the residue stage of both operands with this engine (k_residues_imad / "
                          "k_residues_tc), checked against the other engine")
@@ -49,6 +52,8 @@ def main() -> int:
     with nc.Plan(case.N, case.q_limbs, W=case.W) as plan:
         if a.config:
             plan.row_config = tuple(int(x) for x in a.config.split(","))
+        if a.residue_engine == "imad" or plan.k > 32:
+            plan.residue_engine = nc.RESIDUES_IMAD
         if a.batch > 0:
             with nc.Batch() as batch:
                 for dc in dcs:
