@@ -135,8 +135,6 @@ int nc_plan_set_residue_engine(nc_plan* plan, int engine) {
     return guarded([&] {
         if (!plan) throw nc::Error(nc::kEInval, "null plan");
         if (engine != NC_RESIDUES_IMAD && engine != NC_RESIDUES_TC_I8) throw nc::Error(nc::kEInval, "unknown residue engine");
-        if (engine == NC_RESIDUES_TC_I8 && plan->p->k > nc::kCrtTcMaxPrimes)
-            throw nc::Error(nc::kEInval, "the tensor-core residue stage takes at most 32 primes (q up to about 960 bits)");
         plan->p->res_tc = engine == NC_RESIDUES_TC_I8;
     });
 }
@@ -146,7 +144,7 @@ int nc_plan_get_residue_engine(const nc_plan* plan) {
         nc::set_last_error("null plan");
         return NC_EINVAL;
     }
-    return (plan->p->res_tc && plan->p->k <= nc::kCrtTcMaxPrimes) ? NC_RESIDUES_TC_I8 : NC_RESIDUES_IMAD;
+    return plan->p->res_tc ? NC_RESIDUES_TC_I8 : NC_RESIDUES_IMAD;
 }
 
 int nc_plan_synchronize(nc_plan* plan) {

@@ -86,11 +86,12 @@ void Batch::finalize(cudaStream_t stream) {
     std::vector<BatchProduct> prods(n);
     std::vector<uint64_t> shape;
     size_t scratch = 0;
-    int kmax = 1;
+    int kmax = 1, kmax_imad = 0, kmax_tc = 0;
     for (size_t p = 0; p < n; ++p) {
         const Plan* pl = entries_[p].plan;
         if (!entries_[p].scratch) scratch += 2 * round_up(size_t(pl->k) * pl->N * sizeof(uint64_t), 256);
         kmax = std::max(kmax, pl->k);
+        (pl->res_tc ? kmax_tc : kmax_imad) = std::max(pl->res_tc ? kmax_tc : kmax_imad, pl->k);
     }
     if (scratch > scratch_bytes_) {
         cudaFree(scratch_);
@@ -99,7 +100,7 @@ void Batch::finalize(cudaStream_t stream) {
         check(cudaMalloc(&scratch_, scratch), "batch scratch");
         scratch_bytes_ = scratch;
     }
-    std::vector<uint2> dec, row, crt, crt_tc;
+    std::vector<uint2> dec, row, crt, crt_tc, dec_tc[kMaxLogN1 + 1];
     int lw_tc = 2;
     size_t off = 0;
     char* base = reinterpret_cast<char*>(scratch_);
@@ -126,9 +127,18 @@ void Batch::finalize(cudaStream_t stream) {
         bp.d = d;
         bp.tiles = uint32_t(g.tiles);
         bp.first_operand = e.mode == kModeCachedA ? 1u : 0u;
-        bp.n_dec = uint32_t((e.mode == kModeProduct ? 2 : 1) * g.tiles);
-        bp.n_row = uint32_t(g.row_ctas);
+        bp.tiles_tc = uint32_t(pl->N < kDecTcRows ? 1 : pl->N / kDecTcRows);
+        const uint32_t operands = e.mode == kModeProduct ? 2u : 1u;
         const uint32_t pid = uint32_t(p);
+        if (d.res_tc) {
+            // residues on the tensor cores, in a launch before the persistent one: the product's row
+            // items then wait for no residue item
+            bp.n_dec = 0;
+            for (uint32_t i = 0; i < operands * bp.tiles_tc; ++i) dec_tc[g.logN1].push_back(make_uint2(pid, i));
+        } else {
+            bp.n_dec = operands * uint32_t(g.tiles);
+        }
+        bp.n_row = uint32_t(g.row_ctas);
         for (uint32_t i = 0; i < bp.n_dec; ++i) dec.push_back(make_uint2((kItemDec << 28) | pid, i));
         for (uint32_t i = 0; i < bp.n_row; ++i) row.push_back(make_uint2((kItemRow << 28) | pid, i));
         if (e.mode != kModeForward) {
@@ -150,6 +160,12 @@ void Batch::finalize(cudaStream_t stream) {
     items.insert(items.end(), crt_tc.begin(), crt_tc.end());
     items.insert(items.end(), crt.begin(), crt.end());
     shape.push_back((uint64_t(n_crt_tc_) << 32) | uint64_t(lw_tc));
+    for (int l = 0; l <= kMaxLogN1; ++l) {
+        n_dec_tc_[l] = int(dec_tc[l].size());
+        items.insert(items.end(), dec_tc[l].begin(), dec_tc[l].end());
+        shape.push_back((uint64_t(l) << 32) | uint64_t(n_dec_tc_[l]));
+    }
+    shape.push_back(uint64_t(kmax_tc));
 
     ensure(reinterpret_cast<char**>(&d_products_), &products_cap_, n * sizeof(BatchProduct), "batch products");
     ensure(&d_items_, &items_cap_, items.size(), "batch items");
@@ -178,7 +194,8 @@ void Batch::finalize(cudaStream_t stream) {
         check(cudaMemcpyAsync(d_items_, h_upload_ + prod_bytes, item_bytes, cudaMemcpyHostToDevice, stream), "upload");
     }
 
-    smem_ = smax(dec_smem_bytes(kmax), row_smem_bytes(kThreads, 4));
+    smem_ = smax(kmax_imad > 0 ? dec_smem_bytes(kmax_imad) : 0, row_smem_bytes(kThreads, 4));
+    smem_dec_tc_ = dec_tc_smem_bytes(std::max(kmax_tc, 1));
     smem_crt_ = crt_smem_bytes(kmax);
     smem_crt_tc_ = crt_tc_smem_bytes(lw_tc);
     int per_sm = 0, sms = 0;
@@ -214,9 +231,20 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
     tc.n_items = n_crt_tc_;
     im.items = d_items_ + n_items_ + n_crt_tc_;
     im.n_items = n_crt_;
-    // the persistent launch, then the CRT launches (every row item is done when they start)
+    // the tensor-core residue launches, the persistent launch, then the CRT launches (every row
+    // item is done when they start)
     auto enqueue = [&](cudaStream_t s) -> cudaError_t {
-        cudaError_t e = launch_persistent(args, ctas_, smem_, s);
+        cudaError_t e = cudaSuccess;
+        int at = n_items_ + n_crt_tc_ + n_crt_;
+        for (int l = 0; l <= kMaxLogN1 && e == cudaSuccess; ++l) {
+            if (n_dec_tc_[l] == 0) continue;
+            BatchCrtArgs dt = tc;
+            dt.items = d_items_ + at;
+            dt.n_items = n_dec_tc_[l];
+            e = launch_batch_dec_tc(dt, l, smem_dec_tc_, s);
+            at += n_dec_tc_[l];
+        }
+        if (e == cudaSuccess) e = launch_persistent(args, ctas_, smem_, s);
         if (e == cudaSuccess && n_crt_tc_ > 0) e = launch_batch_crt(tc, true, smem_crt_tc_, s);
         if (e == cudaSuccess && n_crt_ > 0) e = launch_batch_crt(im, false, smem_crt_, s);
         return e;

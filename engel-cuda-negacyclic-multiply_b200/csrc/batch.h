@@ -36,7 +36,11 @@ class Batch {
     void synchronize();
     int ctas() const { return ctas_; }
     size_t scratch_bytes() const { return scratch_bytes_; }
-    int launches_per_run() const { return 1 + (n_crt_tc_ > 0 ? 1 : 0) + (n_crt_ > 0 ? 1 : 0); }
+    int launches_per_run() const {
+        int n = 1 + (n_crt_tc_ > 0 ? 1 : 0) + (n_crt_ > 0 ? 1 : 0);
+        for (int c : n_dec_tc_) n += c > 0 ? 1 : 0;
+        return n;
+    }
     // After the last run has completed (its event): did a dependency wait give up?
     bool failed() const;
     // What the failed wait waited for (empty when nothing failed).
@@ -70,10 +74,12 @@ class Batch {
     size_t scratch_bytes_ = 0;
     int n_items_ = 0;
     int ctas_ = 0;
-    size_t smem_ = 0;      // persistent launch (residue and row items)
+    size_t smem_ = 0;      // persistent launch (row items, and residue items on the integer pipes)
     int n_crt_tc_ = 0;     // CRT items on the tensor cores, after the persistent queue in d_items_
     int n_crt_ = 0;        // CRT items on the integer pipes, after those
     size_t smem_crt_tc_ = 0, smem_crt_ = 0;
+    int n_dec_tc_[kMaxLogN1 + 1] = {};  // tensor-core residue items by log2 N1, after the CRT items
+    size_t smem_dec_tc_ = 0;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
     cudaEvent_t done_ = nullptr;  // recorded after every run

@@ -18,6 +18,8 @@ struct BatchProduct {
     uint32_t n_row;          // row items
     uint32_t tiles;          // residue tiles per operand
     uint32_t first_operand;  // 1 when a is given in the NTT domain (only b is decomposed)
+    uint32_t tiles_tc;       // 128-coefficient tiles per operand (residues on the tensor cores)
+    uint32_t pad;
 };
 
 struct BatchArgs {
@@ -30,7 +32,8 @@ struct BatchArgs {
     Tables tables;
 };
 
-// The CRT launches of a batch: one CTA per item (x = product, y = 256-coefficient tile).
+// The launches of a batch outside the persistent one, one CTA per item: CRT (x = product, y =
+// 256-coefficient tile) and tensor-core residues (x = product, y = operand * tiles_tc + tile).
 struct BatchCrtArgs {
     const BatchProduct* products;
     const uint2* items;

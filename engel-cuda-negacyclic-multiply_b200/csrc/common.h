@@ -133,14 +133,14 @@ NC_HD constexpr size_t crt_tc_smem_bytes(int LW) {
 }
 
 // Residue stage on the tensor cores (plain path): a tile of 128 coefficients (the MMA's M) x 128
-// K bytes of limbs, the weight bytes of up to 32 primes, and p_i; the primes go through the MMA in
-// passes of 16 (128 accumulator columns), so tensor memory holds four CTAs per SM. The shared
-// memory is raised to keep it at four.
+// K bytes of limbs, the weight bytes of the k primes (1 KB each), and p_i; the primes go through
+// the MMA in passes of 16 (128 accumulator columns), so tensor memory holds four CTAs per SM. The
+// shared memory is raised to keep it at four.
 constexpr int kDecTcRows = 128;
 constexpr int kDecTcPassPrimes = 16;
 constexpr uint32_t kDecTcCols = 128;
 NC_HD constexpr size_t dec_tc_smem_bytes(int k) {
-    return smax(size_t(kDecTcRows) * 128 + size_t((k + 1) & ~1) * 1024 + size_t(kCrtTcMaxPrimes) * 8,
+    return smax(size_t(kDecTcRows) * 128 + size_t((k + 1) & ~1) * 1024 + size_t(kMaxPrimes) * 8,
                 (size_t(233472) / (512 / kDecTcCols + 1) + 16) / 16 * 16);
 }
 

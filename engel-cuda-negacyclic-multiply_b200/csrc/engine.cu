@@ -179,7 +179,7 @@ ProductDesc Plan::desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const 
     d.logN2 = uint32_t(cfg.logN2);
     d.crt_b = crt_tc ? d_crt_b : nullptr;
     d.factors = 2;
-    d.res_tc = res_tc && k <= kCrtTcMaxPrimes ? 1u : 0u;
+    d.res_tc = res_tc ? 1u : 0u;
     return d;
 }
 

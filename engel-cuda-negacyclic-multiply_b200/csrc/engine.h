@@ -96,7 +96,7 @@ struct Plan {
     RowConfig cfg{};                 // row-stage tiling of the plain path (autotuned per N)
     uint4* d_crt_b = nullptr;        // byte table of the tensor-core CRT (k <= 32), built at creation
     bool crt_tc = true;              // plain path: CRT accumulation on the tensor cores when available
-    bool res_tc = true;              // plain path: residue stage on the tensor cores when k <= 32
+    bool res_tc = true;              // plain path: residue stage on the tensor cores
     bool timing = false;             // record per-stage events
     cudaEvent_t ev_stage[4] = {nullptr, nullptr, nullptr, nullptr};
 

@@ -1,5 +1,6 @@
-// Stage 1 of the plain path on the tensor cores: k_dec_tc<LOG_N1>, the residues of an operand
-// tile by an exact INT8 contraction, then the forward column stages (the same output as k_dec).
+// Stage 1 on the tensor cores: the residues of an operand tile by an exact INT8 contraction, then
+// the forward column stages (the same output as k_dec); k_dec_tc<LOG_N1> runs one product (plain
+// path), k_batch_dec_tc<LOG_N1> the residue items of a batch.
 //
 // The residue x_n mod p_i of a coefficient given as 4 L bytes x_{n,b} (little-endian limbs, the
 // counterpart of to_residues_tiled_kernel, solve.cu:533-570) is
@@ -8,16 +9,18 @@
 //
 // with w_{i,b,c} byte c of 2^(8 b) mod p_i. S is a u8 x u8 matrix product: 128 coefficients (M)
 // x 128 K bytes (4 L, zero padded) x 8 columns per prime, every S < 128 * 255^2 < 2^23, so the s32
-// accumulation in tensor memory is exact. The primes go through tcgen05.mma kind::i8 in passes of
-// 16 (128 accumulator columns); after each pass the eight warps read the partial sums back
+// accumulation in tensor memory is exact. The primes (any count up to 48) go through
+// tcgen05.mma kind::i8 in passes of 16 (128 accumulator columns); after each pass the eight warps
+// read the partial sums back
 // (tcgen05.ld) and fold sum_c 2^(8 c) S_c (< 2^80) into [0, 2p) modulo p_i. The tile is
 // C = 128 / N1 columns of all N1 rows of the polynomial (row length N2 = N / N1), as in k_dec, so
 // the forward column stages and the residue-row stores follow unchanged.
 //
-// Operand and weight bytes reach shared memory by cp.async (no register staging). The partial
-// sums of pass 0 overwrite the weights of its own primes, those of pass 1 the operand tile, once
-// the pass's MMAs have completed. If the bounded wait for a pass gives up, each warp forms its
+// Operand and weight bytes reach shared memory by cp.async (no register staging). Each prime's
+// residues overwrite its own 1 KB of weights once its pass's MMAs have completed. If the bounded
+// wait for a pass gives up, each warp forms its
 // residues with the integer carry chains of k_dec instead, so the result never depends on it.
+#include "batch_types.h"
 #include "crt_tc.cuh"
 #include "kernel_registry.h"
 
@@ -59,27 +62,19 @@ __device__ __forceinline__ uint64_t fold_planes(const uint32_t* s, uint32_t m) {
     return mad_wide(bq, m, r);
 }
 
-// Residue row of prime i in shared memory (128 values): pass 0's primes over their own weights,
-// pass 1's over the operand tile.
-__device__ __forceinline__ uint64_t* res_row(uint8_t* sA, uint8_t* sB, int i) {
-    return reinterpret_cast<uint64_t*>(i < kDecTcPassPrimes ? sB + i * 1024 : sA + (i - kDecTcPassPrimes) * 1024);
-}
+// Residue row of prime i in shared memory (128 values), over the prime's own weights.
+__device__ __forceinline__ uint64_t* res_row(uint8_t* sB, int i) { return reinterpret_cast<uint64_t*>(sB + i * 1024); }
 
 // Slot of tile row x in prime i's residue row: rows XORed with (i C) mod 16, so that the 32 / C
 // primes one warp reads in the column stages (C consecutive rows each) fall on different banks.
 __device__ __forceinline__ int res_slot(int i, int x, int C) { return x ^ ((i * C) & 15); }
 
-// Four CTAs per SM where the column transform fits 64 registers; the 16- and 32-point columns
-// (N1 values per thread) take three and two.
+// One CTA's tile: operand `operand` of product d, 128-coefficient tile `tile`; `bar` and
+// `taddr_slot` are the CTA's mbarrier and tensor-memory address slot in shared memory.
 template <int LOG_N1>
-__global__ void __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 2))
-    k_dec_tc(ProductDesc d, Tables t, int first_operand, int tiles) {
+__device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& t, int operand, int tile, uint8_t* smem,
+                                            uint64_t& bar, uint32_t& taddr_slot) {
     constexpr int N1 = 1 << LOG_N1;
-    extern __shared__ __align__(16) uint8_t smem[];
-    __shared__ uint64_t bar;
-    __shared__ uint32_t taddr_slot;
-    const int operand = first_operand + int(blockIdx.x) / tiles;
-    const int tile = int(blockIdx.x) % tiles;
     const int N = 1 << d.logN;
     const int N2 = N >> LOG_N1;
     const int T = N < kDecTcRows ? N : kDecTcRows;
@@ -183,9 +178,9 @@ __global__ void __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 
                       "=r"(s[15])
                     : "r"(lane_base + uint32_t(8 * (i - i0))));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                res_row(sA, sB, i)[res_slot(i, m, C)] = fold_planes(s, uint32_t((uint64_t(1) << 62) - s_p[i]));
+                res_row(sB, i)[res_slot(i, m, C)] = fold_planes(s, uint32_t((uint64_t(1) << 62) - s_p[i]));
                 if (i + 1 < ie)
-                    res_row(sA, sB, i + 1)[res_slot(i + 1, m, C)] =
+                    res_row(sB, i + 1)[res_slot(i + 1, m, C)] =
                         fold_planes(s + 8, uint32_t((uint64_t(1) << 62) - s_p[i + 1]));
             }
         } else if (m < T) {
@@ -198,7 +193,7 @@ __global__ void __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 
                     const uint64_t c = __ldg(t.pow32 + size_t(i) * kMaxL + l);
                     mac_u32x64(__ldg(row + l), uint32_t(c), uint32_t(c >> 32), a0, a1, a2, b0, b1, b2);
                 }
-                res_row(sA, sB, i)[res_slot(i, m, C)] =
+                res_row(sB, i)[res_slot(i, m, C)] =
                     reduce_limb_sum(a0, a1, a2, b0, b1, b2, (uint64_t(1) << 62) - s_p[i]);
             }
         }
@@ -212,7 +207,7 @@ __global__ void __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 
     // forward column stages of items (prime i, column j), then the residue rows
     for (int w = tid; w < k * C; w += kThreads) {
         const int i = w >> logC, j = w & (C - 1);
-        const uint64_t* sr = res_row(sA, sB, i);
+        const uint64_t* sr = res_row(sB, i);
         uint64_t v[N1];
 #pragma unroll
         for (int u = 0; u < N1; ++u) v[u] = sr[res_slot(i, u * C + j, C)];
@@ -220,6 +215,45 @@ __global__ void __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 
         uint64_t* out = R + size_t(i) * N + j0 + j;
 #pragma unroll
         for (int u = 0; u < N1; ++u) __stcg(out + size_t(u) * N2, v[u]);
+    }
+}
+
+// Four CTAs per SM where the column transform fits 64 registers; the 16- and 32-point columns
+// (N1 values per thread) take three and two.
+#define NC_DEC_TC_BOUNDS(LOG_N1) __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 2))
+
+// Plain path: one product, grid = operands x tiles.
+template <int LOG_N1>
+__global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_dec_tc(ProductDesc d, Tables t, int first_operand, int tiles) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t taddr_slot;
+    dec_tc_item<LOG_N1>(d, t, first_operand + int(blockIdx.x) / tiles, int(blockIdx.x) % tiles, smem, bar, taddr_slot);
+}
+
+// Batches: one CTA per item (x = product, y = operand * tiles + tile), every product of the launch
+// with the same column length N1.
+template <int LOG_N1>
+__global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_batch_dec_tc(BatchCrtArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t taddr_slot;
+    const uint2 w = __ldg(a.items + blockIdx.x);
+    const BatchProduct& bp = a.products[w.x];
+    const int tiles = int(bp.tiles_tc);
+    dec_tc_item<LOG_N1>(bp.d, a.tables, int(bp.first_operand) + int(w.y) / tiles, int(w.y) % tiles, smem, bar,
+                        taddr_slot);
+}
+
+void* batch_dec_tc_kernel(int logN1) {
+    switch (logN1) {
+        case 0: return reinterpret_cast<void*>(&k_batch_dec_tc<0>);
+        case 1: return reinterpret_cast<void*>(&k_batch_dec_tc<1>);
+        case 2: return reinterpret_cast<void*>(&k_batch_dec_tc<2>);
+        case 3: return reinterpret_cast<void*>(&k_batch_dec_tc<3>);
+        case 4: return reinterpret_cast<void*>(&k_batch_dec_tc<4>);
+        case 5: return reinterpret_cast<void*>(&k_batch_dec_tc<5>);
+        default: return nullptr;
     }
 }
 
@@ -239,10 +273,23 @@ void* dec_tc_kernel(int logN1) {
 
 cudaError_t prepare_dec_tc(const PrimeConst* pc, const uint64_t* pow32) {
     cudaError_t e = upload_prime_constants(pc, pow32);
-    for (int l = 0; l <= kMaxLogN1 && e == cudaSuccess; ++l)
+    for (int l = 0; l <= kMaxLogN1 && e == cudaSuccess; ++l) {
         e = cudaFuncSetAttribute(dec_tc_kernel(l), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(dec_tc_smem_bytes(kCrtTcMaxPrimes)));
+                                 int(dec_tc_smem_bytes(kMaxPrimes)));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(batch_dec_tc_kernel(l), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(dec_tc_smem_bytes(kMaxPrimes)));
+    }
     return e;
+}
+
+cudaError_t launch_batch_dec_tc(const BatchCrtArgs& args, int logN1, size_t smem, cudaStream_t s) {
+    void* fn = batch_dec_tc_kernel(logN1);
+    if (!fn) return cudaErrorInvalidValue;
+    if (args.n_items <= 0) return cudaSuccess;
+    BatchCrtArgs a = args;
+    void* params[] = {&a};
+    return cudaLaunchKernel(fn, dim3(unsigned(args.n_items)), dim3(kThreads), params, smem, s);
 }
 
 }  // namespace nc

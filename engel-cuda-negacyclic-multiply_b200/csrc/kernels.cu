@@ -59,7 +59,7 @@ cudaError_t launch_residues(const ProductDesc& d, const Tables& t, const RowConf
                             int count) {
     ProductDesc dd = d;
     Tables tt = t;
-    if (d.res_tc && int(d.k) <= kCrtTcMaxPrimes && t.res_w) {
+    if (d.res_tc && t.res_w) {
         // tensor-core residues: 128-coefficient tiles
         void* dec = dec_tc_kernel(int(d.logN) - cfg.logN2);
         if (!dec) return cudaErrorInvalidValue;

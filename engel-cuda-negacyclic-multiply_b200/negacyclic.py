@@ -221,7 +221,7 @@ class Plan:
 
     @property
     def residue_engine(self) -> int:
-        """RESIDUES_TC_I8 (default with at most 32 primes) or RESIDUES_IMAD for this plan's products."""
+        """RESIDUES_TC_I8 (the default) or RESIDUES_IMAD for this plan's products."""
         e = load().nc_plan_get_residue_engine(self._h)
         if e < 0:
             _check(e)

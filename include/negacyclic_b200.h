@@ -145,8 +145,8 @@ int nc_residues_status(int* gave_up);
 
 /* Engine of the residue stage of the plan's own products (nc_multiply, nc_multiply_device, the
    chained products; batches and servers keep the integer pipes inside their persistent launch):
-     NC_RESIDUES_TC_I8  the default when the plan has at most 32 primes: the contraction above on
-                        128-coefficient tiles, fused with the forward column stages (k_dec_tc);
+     NC_RESIDUES_TC_I8  the default: the contraction above on 128-coefficient tiles, in passes of
+                        16 primes (any prime count), fused with the forward column stages (k_dec_tc);
      NC_RESIDUES_IMAD   the integer-pipe residue stage (k_dec; always available).
    Both give the same residues mod p_i and so the same product. Set it only while no product of
    the plan is in flight; nc_plan_get_residue_engine returns the engine in use. */

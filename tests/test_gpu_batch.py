@@ -140,3 +140,51 @@ def test_batch_replay_with_new_operands(gpu):
             outs.append(_host(dc))
         for c, o in zip((c1, c2), outs):
             assert np.array_equal(o, oracle.negacyclic(N, c.q_limbs, c.a, c.b))
+
+
+def test_batch_mixes_residue_engines(gpu):
+    """One batch with tensor-core residue items (one launch per column length N1: N from 2^6 to
+    2^16), products on the integer residue stage (inside the persistent launch), a forward-mode
+    item and a cached-a item: every product matches the oracle, in two graph replays."""
+    import torch
+
+    specs = [(64, 868, nc.RESIDUES_TC_I8), (8192, 434, nc.RESIDUES_TC_I8), (16384, 868, nc.RESIDUES_IMAD),
+             (32768, 600, nc.RESIDUES_TC_I8), (65536, 868, nc.RESIDUES_TC_I8), (4096, 1000, nc.RESIDUES_IMAD),
+             (2048, 1024, nc.RESIDUES_TC_I8)]
+    plans, bufs, want = [], [], []
+    try:
+        with nc.Batch() as batch:
+            for i, (N, bits, engine) in enumerate(specs):
+                c = cases.make_case(N, bits, seed=950 + i, edge_frac=0.02)
+                p = nc.Plan(N, c.q_limbs)
+                p.residue_engine = engine
+                plans.append(p)
+                da, db = _dev(c.a, gpu), _dev(c.b, gpu)
+                dc = da.new_zeros(da.shape)
+                batch.add(p, da.data_ptr(), db.data_ptr(), dc.data_ptr())
+                bufs.append((da, db, dc))
+                want.append(oracle.negacyclic(N, c.q_limbs, c.a, c.b))
+            # a cached-a product whose a_hat comes from a forward item of an earlier batch
+            c = cases.make_case(16384, 868, seed=960, edge_frac=0.02)
+            p = nc.Plan(16384, c.q_limbs)
+            plans.append(p)
+            da, db = _dev(c.a, gpu), _dev(c.b, gpu)
+            ahat = torch.empty(p.hat_words, dtype=torch.int64, device=gpu)
+            with nc.Batch() as fwd:
+                fwd.add_forward(p, da.data_ptr(), ahat.data_ptr())
+                fwd.run(0, True)
+                fwd.synchronize()
+            dc = da.new_zeros(da.shape)
+            batch.add_cached(p, ahat.data_ptr(), db.data_ptr(), dc.data_ptr())
+            bufs.append((da, db, dc))
+            want.append(oracle.negacyclic(16384, c.q_limbs, c.a, c.b))
+            for _ in range(2):
+                for _, _, out in bufs:
+                    out.zero_()
+                batch.run(0, True)
+                batch.synchronize()
+                for (_, _, out), w in zip(bufs, want):
+                    assert np.array_equal(_host(out), w)
+    finally:
+        for p in plans:
+            p.close()

@@ -1,7 +1,8 @@
-"""The residue stage of the plan's own products on the tensor cores (k_dec_tc, default for <= 32
-primes) and on the integer pipes (k_dec): both give the oracle's product bit for bit, for every
-operand load width (L a multiple of 4, even, odd), partial tiles (N < 128), every column-transform
-length N1 = 1 .. 32 (row configurations), the host path and chained products."""
+"""The residue stage of the plan's own products on the tensor cores (k_dec_tc, the default) and on
+the integer pipes (k_dec): both give the oracle's product bit for bit, for every operand load width
+(L a multiple of 4, even, odd), partial tiles (N < 128), every column-transform length N1 = 1 .. 32
+(row configurations), one to three MMA passes (up to 48 primes), the host path and chained
+products."""
 from __future__ import annotations
 
 import numpy as np
@@ -85,12 +86,25 @@ def test_device_path_and_chain(gpu):
         assert np.array_equal(out.cpu().numpy().view(np.uint32).reshape(N, -1), want)
 
 
-def test_engine_limits(gpu):
-    q = cases.gen_prime(1024, 84)
-    with nc.Plan(256, cases.limbs_of(q, 32)) as plan:
-        assert plan.k > 32 and plan.residue_engine == nc.RESIDUES_IMAD
+@pytest.mark.parametrize("N,bits,m", [(256, 1024, 2), (4096, 1000, 2), (16384, 868, 3), (1024, 731, 4)])
+def test_beyond_32_primes(gpu, N, bits, m):
+    """33 to 48 primes (three MMA passes): wide q and chained products."""
+    c = cases.make_case(N, bits, seed=85 + N + bits, edge_frac=0.02)
+    xs = [c.a, c.b] + [cases.coeffs(c.q, N, c.L, 86 + f) for f in range(m - 2)]
+    want = xs[0]
+    for x in xs[1:]:
+        want = oracle.negacyclic(N, c.q_limbs, want, x)
+    with nc.Plan(N, c.q_limbs, factors=m) as plan:
+        assert plan.k > 32 and plan.residue_engine == nc.RESIDUES_TC_I8
+        for engine in (nc.RESIDUES_TC_I8, nc.RESIDUES_IMAD):
+            plan.residue_engine = engine
+            got = plan.multiply_chain(xs) if m > 2 else plan.multiply(xs[0], xs[1])
+            assert np.array_equal(got, want), engine
+
+
+def test_unknown_engine_rejected(gpu):
+    c = cases.make_case(64, 434, seed=87)
+    with nc.Plan(64, c.q_limbs) as plan:
         with pytest.raises(nc.NegacyclicError) as ei:
-            plan.residue_engine = nc.RESIDUES_TC_I8
-        assert ei.value.code == nc.NC_EINVAL
-        with pytest.raises(nc.NegacyclicError):
             plan.residue_engine = 7
+        assert ei.value.code == nc.NC_EINVAL
