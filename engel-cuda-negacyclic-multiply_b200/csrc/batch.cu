@@ -29,9 +29,15 @@ void ensure(T** p, size_t* cap, size_t count, const char* what) {
 Batch::Batch(int device) : device_(device) {
     tables_ = acquire_tables(device);
     cudaError_t e = cudaEventCreateWithFlags(&done_, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join_, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost(&err_host_, 4 * sizeof(uint32_t));
     if (e != cudaSuccess) {
         if (done_) cudaEventDestroy(done_);
+        if (fork_) cudaEventDestroy(fork_);
+        if (join_) cudaEventDestroy(join_);
+        if (side_) cudaStreamDestroy(side_);
         release_tables(tables_);
         check(e, "batch event");
     }
@@ -44,6 +50,9 @@ Batch::~Batch() {
     // wait on the batch's own event (never on the caller's stream, which may be gone)
     if (ran_) cudaEventSynchronize(done_);
     cudaEventDestroy(done_);
+    cudaEventDestroy(fork_);
+    cudaEventDestroy(join_);
+    cudaStreamDestroy(side_);
     cudaFreeHost(err_host_);
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
@@ -101,6 +110,7 @@ void Batch::finalize(cudaStream_t stream) {
         scratch_bytes_ = scratch;
     }
     std::vector<uint2> dec, row, crt, crt_tc, dec_tc[kMaxLogN1 + 1];
+    direct_.clear();
     int lw_tc = 2;
     size_t off = 0;
     char* base = reinterpret_cast<char*>(scratch_);
@@ -122,6 +132,15 @@ void Batch::finalize(cudaStream_t stream) {
             d.ra = reinterpret_cast<uint64_t*>(base + off);
             d.rb = reinterpret_cast<uint64_t*>(base + off + res);
             off += 2 * res;
+        }
+        if (pl->logN >= kDirectLogN) {
+            // fills the GPU alone: the plain path's launches with the plan's row configuration
+            d.logN2 = uint32_t(pl->cfg.logN2);
+            direct_.push_back(Direct{d, pl->cfg});
+            shape.push_back((uint64_t(1) << 63) | (uint64_t(pl->logN) << 40) | (uint64_t(pl->k) << 32) |
+                            (uint64_t(pl->cfg.logN2) << 24) | (uint64_t(pl->cfg.logE) << 16) |
+                            (uint64_t(pl->cfg.threads) << 4) | e.mode);
+            continue;
         }
         BatchProduct& bp = prods[p];
         bp.d = d;
@@ -235,6 +254,13 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
     // item is done when they start)
     auto enqueue = [&](cudaStream_t s) -> cudaError_t {
         cudaError_t e = cudaSuccess;
+        if (!direct_.empty()) {
+            // direct products alternate between s and the side stream (forked from s, joined below)
+            e = cudaEventRecord(fork_, s);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(side_, fork_, 0);
+            for (size_t j = 0; j < direct_.size() && e == cudaSuccess; ++j)
+                e = launch_product(direct_[j].d, args.tables, direct_[j].cfg, (j & 1) ? side_ : s);
+        }
         int at = n_items_ + n_crt_tc_ + n_crt_;
         for (int l = 0; l <= kMaxLogN1 && e == cudaSuccess; ++l) {
             if (n_dec_tc_[l] == 0) continue;
@@ -244,9 +270,15 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
             e = launch_batch_dec_tc(dt, l, smem_dec_tc_, s);
             at += n_dec_tc_[l];
         }
-        if (e == cudaSuccess) e = launch_persistent(args, ctas_, smem_, s);
+        if (e == cudaSuccess && n_items_ > 0) e = launch_persistent(args, ctas_, smem_, s);
         if (e == cudaSuccess && n_crt_tc_ > 0) e = launch_batch_crt(tc, true, smem_crt_tc_, s);
         if (e == cudaSuccess && n_crt_ > 0) e = launch_batch_crt(im, false, smem_crt_, s);
+        if (!direct_.empty()) {
+            // join the side stream back into s (also after a failed launch, so a capture ends whole)
+            cudaError_t j = cudaEventRecord(join_, side_);
+            if (j == cudaSuccess) j = cudaStreamWaitEvent(s, join_, 0);
+            if (e == cudaSuccess) e = j;
+        }
         return e;
     };
     const size_t state_bytes = (2 * n + 5) * sizeof(uint32_t);

@@ -13,10 +13,13 @@ namespace nc {
 
 
 // A list of products (each referring to a plan for its q, N and constants) that run together.
-// Products may differ in N and in q. Residue scratch comes from the batch's own arena. A run is
-// one persistent launch for the residue and row stages of every product, then one CRT launch per
-// CRT engine in use; the counter reset and the launches are captured once into a CUDA graph and
-// replayed while the batch keeps the same shape.
+// Products may differ in N and in q. Residue scratch comes from the batch's own arena. A run is,
+// for products below N = 2^15: the tensor-core residue launches, one persistent launch for the
+// row stage (and any residue items on the integer pipes), then one CRT launch per CRT engine in
+// use. Products of N >= 2^15 fill the GPU on their own: they run the plain path's launches with
+// their plan's row configuration, alternating between two streams so that one product's last
+// wave overlaps the next one's kernels. The counter reset and the launches are captured once into
+// a CUDA graph and replayed while the batch keeps the same shape.
 class Batch {
   public:
     explicit Batch(int device);
@@ -37,8 +40,9 @@ class Batch {
     int ctas() const { return ctas_; }
     size_t scratch_bytes() const { return scratch_bytes_; }
     int launches_per_run() const {
-        int n = 1 + (n_crt_tc_ > 0 ? 1 : 0) + (n_crt_ > 0 ? 1 : 0);
+        int n = (n_items_ > 0 ? 1 : 0) + (n_crt_tc_ > 0 ? 1 : 0) + (n_crt_ > 0 ? 1 : 0);
         for (int c : n_dec_tc_) n += c > 0 ? 1 : 0;
+        for (const Direct& x : direct_) n += x.d.mode == kModeForward ? 2 : 3;
         return n;
     }
     // After the last run has completed (its event): did a dependency wait give up?
@@ -57,8 +61,17 @@ class Batch {
         uint64_t* hat_out;
         uint64_t* scratch;
     };
+    // A product of N >= 2^15, launched as on the plain path.
+    struct Direct {
+        ProductDesc d;
+        RowConfig cfg;
+    };
+    static constexpr int kDirectLogN = 15;
     void finalize(cudaStream_t stream);
     int device_;
+    std::vector<Direct> direct_;
+    cudaStream_t side_ = nullptr;                    // second stream of the direct products
+    cudaEvent_t fork_ = nullptr, join_ = nullptr;
     std::vector<Entry> entries_;
     std::vector<uint64_t> shape_;  // signature of the captured graph
     DeviceTables* tables_ = nullptr;
