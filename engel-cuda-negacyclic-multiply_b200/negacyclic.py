@@ -296,8 +296,9 @@ def row_variants(log_n: int) -> list[tuple[int, int, int]]:
 
 
 class Batch:
-    """Many products (any mix of plans) in one persistent launch for residues and rows plus one CRT
-    launch per engine (nc_batch_*). Device pointers."""
+    """Many products (any mix of plans) run together (nc_batch_*): tensor-core residue launches, one
+    persistent launch for the row stage, one CRT launch per engine; products of N >= 2^15 as plain
+    launches on two graph branches. Device pointers."""
 
     def __init__(self):
         self._h = _vp()

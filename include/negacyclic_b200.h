@@ -143,8 +143,8 @@ int nc_residues(const nc_plan* plan, const uint32_t* d_x, uint64_t* d_r, int eng
    its bounded wait for the MMA (its residues are then not written); the flag is cleared. */
 int nc_residues_status(int* gave_up);
 
-/* Engine of the residue stage of the plan's own products (nc_multiply, nc_multiply_device, the
-   chained products; batches and servers keep the integer pipes inside their persistent launch):
+/* Engine of the residue stage of the plan's products (nc_multiply, nc_multiply_device, the chained
+   products, and the plan's products in batches and servers):
      NC_RESIDUES_TC_I8  the default: the contraction above on 128-coefficient tiles, in passes of
                         16 primes (any prime count), fused with the forward column stages (k_dec_tc);
      NC_RESIDUES_IMAD   the integer-pipe residue stage (k_dec; always available).
@@ -170,12 +170,15 @@ int nc_plan_autotune(nc_plan* plan, int reps, float* best_ms);
 
 /* ------------------------------------------------------------------ batches
  *
- * A batch runs many products, of any mix of N and q (one plan each), in one persistent kernel
- * launch for the residue and row stages (per-tile and per-(prime, row block) work items in a
- * global queue, dependency counters per product, bounded waits), followed by one CRT launch per
- * CRT engine in use (one CTA per product tile). The counter reset and the launches are captured
- * into a CUDA graph and replayed while the batch keeps its shape. Device buffers are 16-byte
- * aligned and must stay valid until the batch has run. */
+ * A batch runs many products, of any mix of N and q (one plan each). Products below N = 2^15:
+ * the tensor-core residue items in one launch per column length, then one persistent kernel
+ * launch for the row stage (per-(prime, row block) work items in a global queue, with the residue
+ * items of products on the integer residue engine and dependency counters per product, bounded
+ * waits), then one CRT launch per CRT engine in use (one CTA per product tile). Products of
+ * N >= 2^15 run the plain path's launches with their plan's row configuration, alternating
+ * between two streams so that consecutive products overlap. The counter reset and the launches
+ * are captured into a CUDA graph and replayed while the batch keeps its shape. Device buffers are
+ * 16-byte aligned and must stay valid until the batch has run. */
 
 typedef struct nc_batch nc_batch;
 
