@@ -65,6 +65,43 @@ __device__ void crt_columns_tc(const ProductDesc& d, const Tables& t, int j0, in
     const int N2 = N >> LOG_N1;
     const int C = T >> LOG_N1;
     const int k = int(d.k);
+    if constexpr (LOG_N1 == 5) {
+        // 32-point columns on two adjacent lanes: lane h loads rows [16h, 16h + 16) and runs the
+        // inverse stages of its half-subtree (twiddle root 2 + h); then the last stage's pairs
+        // (u, u + 16) are split between the lanes (lane 0: u < 8, lane 1: 8 <= u < 16) with one
+        // exchange of eight values. Pairs never straddle a warp (2 k C is even).
+        const int total = 2 * k * C;
+        const int lane = int(threadIdx.x) & 31;
+        for (int w0 = int(threadIdx.x) & ~31; w0 < total; w0 += int(blockDim.x)) {
+            const int w = w0 + lane;
+            const bool active = w < total;
+            const int item = active ? w >> 1 : 0, h = w & 1;
+            const int i = item / C, j = item - i * C;
+            const uint64_t* row = d.ra + size_t(i) * N + j0 + j + size_t(16 * h) * N2;
+            uint64_t v[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) v[u] = active ? __ldcg(row + size_t(u) * N2) : 0;
+            const uint64_t p = s_p[i], p2 = 2 * p;
+            const ulonglong2* tw = t.inv + size_t(i) * kMaxN;
+            column_inverse_root<4>(tw, 2 + h, p, v);
+            const ulonglong2 w1 = __ldg(tw + 1);
+            const uint64_t y = s_y[i], ys = s_ys[i];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const uint64_t got = shfl_pair(h ? v[e] : v[8 + e]);
+                uint64_t lo = h ? got : v[e], hi = h ? v[8 + e] : got;  // rows 8h + e and 8h + e + 16
+                gs_bfly(lo, hi, w1.x, w1.y, p, p2);
+                if (active) {
+                    const int tl = (8 * h + e) * C + j, th = (8 * h + e + 16) * C + j;
+                    *reinterpret_cast<uint64_t*>(sA + (tl >> 7) * kCrtTcHalfBytes + a_offset(tl & 127, 8 * i)) =
+                        csub(shoup_lazy(lo, y, ys, p), p);
+                    *reinterpret_cast<uint64_t*>(sA + (th >> 7) * kCrtTcHalfBytes + a_offset(th & 127, 8 * i)) =
+                        csub(shoup_lazy(hi, y, ys, p), p);
+                }
+            }
+        }
+        return;
+    }
     for (int w = threadIdx.x; w < k * C; w += blockDim.x) {
         const int i = w / C, j = w - i * C;
         const uint64_t* row = d.ra + size_t(i) * N + j0 + j;

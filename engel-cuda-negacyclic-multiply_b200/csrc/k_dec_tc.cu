@@ -205,22 +205,65 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kDecTcCols) : "memory");
 
     // forward column stages of items (prime i, column j), then the residue rows
-    for (int w = tid; w < k * C; w += kThreads) {
-        const int i = w >> logC, j = w & (C - 1);
-        const uint64_t* sr = res_row(sB, i);
-        uint64_t v[N1];
+    if constexpr (LOG_N1 == 5) {
+        // 32-point columns on two adjacent lanes (16 values each, like the 16-point case): lane h
+        // runs the first stage's butterflies (u, u + 16) for u in [8h, 8h + 8), the lanes swap
+        // halves so that lane h holds rows [16h, 16h + 16), and each runs the four remaining stages
+        // on its half-subtree (twiddle root 2 + h). Pairs never straddle a warp (2 k C is even).
+        const int total = 2 * k * C;
+        for (int w0 = tid & ~31; w0 < total; w0 += kThreads) {
+            const int w = w0 + lane;
+            const bool active = w < total;
+            const int item = active ? w >> 1 : 0, h = w & 1;
+            const int i = item >> logC, j = item & (C - 1);
+            const uint64_t* sr = res_row(sB, i);
+            const uint64_t p = s_p[i], p2 = 2 * p;
+            const ulonglong2* tw = t.fwd + size_t(i) * kMaxN;
+            uint64_t x[8], y[8];
+            const ulonglong2 w1 = __ldg(tw + 1);
 #pragma unroll
-        for (int u = 0; u < N1; ++u) v[u] = sr[res_slot(i, u * C + j, C)];
-        if (LOG_N1 > 0) column_forward<LOG_N1>(t.fwd + size_t(i) * kMaxN, s_p[i], v);
-        uint64_t* out = R + size_t(i) * N + j0 + j;
+            for (int e = 0; e < 8; ++e) {
+                const int u = 8 * h + e;
+                x[e] = sr[res_slot(i, u * C + j, C)];
+                y[e] = sr[res_slot(i, (u + 16) * C + j, C)];
+                ct_bfly(x[e], y[e], w1.x, w1.y, p, p2);
+            }
+            // lane 0 keeps x (rows 0..7) and takes lane 1's x (8..15); lane 1 takes lane 0's y
+            // (16..23) and keeps y (24..31)
+            uint64_t v[16];
 #pragma unroll
-        for (int u = 0; u < N1; ++u) __stcg(out + size_t(u) * N2, v[u]);
+            for (int e = 0; e < 8; ++e) {
+                const uint64_t send = h ? x[e] : y[e];
+                const uint64_t got = (uint64_t(__shfl_xor_sync(0xffffffffu, uint32_t(send >> 32), 1)) << 32) |
+                                     __shfl_xor_sync(0xffffffffu, uint32_t(send), 1);
+                v[e] = h ? got : x[e];
+                v[8 + e] = h ? y[e] : got;
+            }
+            column_forward_root<4>(tw, 2 + h, p, v);
+            if (active) {
+                uint64_t* out = R + size_t(i) * N + j0 + j + size_t(16 * h) * N2;
+#pragma unroll
+                for (int u = 0; u < 16; ++u) __stcg(out + size_t(u) * N2, v[u]);
+            }
+        }
+    } else {
+        for (int w = tid; w < k * C; w += kThreads) {
+            const int i = w >> logC, j = w & (C - 1);
+            const uint64_t* sr = res_row(sB, i);
+            uint64_t v[N1];
+#pragma unroll
+            for (int u = 0; u < N1; ++u) v[u] = sr[res_slot(i, u * C + j, C)];
+            if (LOG_N1 > 0) column_forward<LOG_N1>(t.fwd + size_t(i) * kMaxN, s_p[i], v);
+            uint64_t* out = R + size_t(i) * N + j0 + j;
+#pragma unroll
+            for (int u = 0; u < N1; ++u) __stcg(out + size_t(u) * N2, v[u]);
+        }
     }
 }
 
-// Four CTAs per SM where the column transform fits 64 registers; the 16- and 32-point columns
-// (N1 values per thread) take three and two.
-#define NC_DEC_TC_BOUNDS(LOG_N1) __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : (LOG_N1 == 4 ? 3 : 2))
+// Four CTAs per SM where the column transform fits 64 registers; 16 values per thread (16-point
+// columns, and 32-point columns on two lanes) take three.
+#define NC_DEC_TC_BOUNDS(LOG_N1) __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : 3)
 
 // Plain path: one product, grid = operands x tiles.
 template <int LOG_N1>

@@ -136,6 +136,29 @@ __device__ __forceinline__ void column_forward(const ulonglong2* tw, uint64_t p,
     }
 }
 
+// The same stages on one half-subtree of a longer column: the 2^LOG_N1 values under node `root`
+// of the merged twiddle tree (the full column is root 1), whose stage s uses twiddle
+// (root << s) + block.
+template <int LOG_N1>
+__device__ __forceinline__ void column_forward_root(const ulonglong2* tw, int root, uint64_t p,
+                                                    uint64_t (&v)[1 << LOG_N1]) {
+    constexpr int N1 = 1 << LOG_N1;
+    const uint64_t p2 = 2 * p;
+#pragma unroll
+    for (int s = 0; s < LOG_N1; ++s) {
+        const int half = N1 >> (s + 1);
+#pragma unroll
+        for (int blk = 0; blk < (1 << s); ++blk) {
+            const ulonglong2 w = __ldg(tw + (root << s) + blk);
+#pragma unroll
+            for (int jj = 0; jj < half; ++jj) {
+                const int u = blk * 2 * half + jj;
+                ct_bfly(v[u], v[u + half], w.x, w.y, p, p2);
+            }
+        }
+    }
+}
+
 // Inverse column stages (global stages m = N1/2 .. 1) of one column held in registers.
 template <int LOG_N1>
 __device__ __forceinline__ void column_inverse(const ulonglong2* tw, uint64_t p, uint64_t (&v)[1 << LOG_N1]) {
@@ -154,6 +177,33 @@ __device__ __forceinline__ void column_inverse(const ulonglong2* tw, uint64_t p,
             }
         }
     }
+}
+
+// Inverse stages of one half-subtree of a longer column (root as in column_forward_root).
+template <int LOG_N1>
+__device__ __forceinline__ void column_inverse_root(const ulonglong2* tw, int root, uint64_t p,
+                                                    uint64_t (&v)[1 << LOG_N1]) {
+    constexpr int N1 = 1 << LOG_N1;
+    const uint64_t p2 = 2 * p;
+#pragma unroll
+    for (int s = LOG_N1 - 1; s >= 0; --s) {
+        const int half = N1 >> (s + 1);
+#pragma unroll
+        for (int blk = 0; blk < (1 << s); ++blk) {
+            const ulonglong2 w = __ldg(tw + (root << s) + blk);
+#pragma unroll
+            for (int jj = 0; jj < half; ++jj) {
+                const int u = blk * 2 * half + jj;
+                gs_bfly(v[u], v[u + half], w.x, w.y, p, p2);
+            }
+        }
+    }
+}
+
+// A u64 from the neighbouring lane (lane ^ 1) of a full warp.
+__device__ __forceinline__ uint64_t shfl_pair(uint64_t x) {
+    return (uint64_t(__shfl_xor_sync(0xffffffffu, uint32_t(x >> 32), 1)) << 32) |
+           __shfl_xor_sync(0xffffffffu, uint32_t(x), 1);
 }
 
 // Items (prime i, column j) of the tile: column transform from s_res, store the residue rows.
