@@ -65,6 +65,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched / uneven / serving sections")
+    ap.add_argument("--row-config", type=str, default="",
+                    help="pin the row configuration (log_block,log_radix,threads) instead of autotuning, e.g. to "
+                         "profile the configuration a plain run picked")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.steps = max(a.steps, 1)
@@ -276,7 +279,11 @@ def ours(args) -> dict | None:
 
     case = cases.make_case(N_MAIN, BITS, SEED, edge_frac=EDGE)
     plan = nc.Plan(case.N, case.q_limbs, W=case.W)
-    tuned_ms = plan.autotune(reps=3)  # untimed: picks the row tiling for N = 65536
+    if args.row_config:
+        plan.row_config = tuple(int(x) for x in args.row_config.split(","))
+        tuned_ms = None
+    else:
+        tuned_ms = plan.autotune(reps=3)  # untimed: picks the row tiling for N = 65536
     # the timed steps run the product as a caller does (no per-stage events: they cost ~10 us a
     # product); the per-stage split comes from a separate pass afterwards
     plan.set_timing(False)
