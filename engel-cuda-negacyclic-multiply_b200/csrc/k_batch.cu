@@ -1,5 +1,7 @@
-// Batched kernels: every product of a batch in one persistent launch for the residue and row
-// stages, then the CRT stage of every product in one launch per CRT engine.
+// Batched kernels: the row stage of every product of a batch (and the residue stage of products on
+// the integer residue engine) in one persistent launch, then the CRT stage of every product in one
+// launch per CRT engine. Residues on the tensor cores run before, in k_batch_dec_tc (k_dec_tc.cu);
+// products of N >= 2^15 take the plain path's launches instead (batch.cu).
 //
 // Persistent launch: the host lays out a work queue of items (stage, product, index): all residue
 // items of every product, then all row items. CTAs (as many as fit on the GPU at once) take items
