@@ -117,7 +117,7 @@ void Batch::finalize(cudaStream_t stream) {
     for (size_t p = 0; p < n; ++p) {
         const Entry& e = entries_[p];
         const Plan* pl = e.plan;
-        const RowConfig cfg = default_row_config(pl->logN);
+        const RowConfig cfg = batch_row_config(pl->logN);
         const Geometry g = geometry(pl->logN, pl->k, cfg);
         ProductDesc d = pl->desc(e.a, e.b, e.c);
         d.logN2 = uint32_t(cfg.logN2);
@@ -213,7 +213,7 @@ void Batch::finalize(cudaStream_t stream) {
         check(cudaMemcpyAsync(d_items_, h_upload_ + prod_bytes, item_bytes, cudaMemcpyHostToDevice, stream), "upload");
     }
 
-    smem_ = smax(kmax_imad > 0 ? dec_smem_bytes(kmax_imad) : 0, row_smem_bytes(kThreads, 4));
+    smem_ = smax(kmax_imad > 0 ? dec_smem_bytes(kmax_imad) : 0, row_smem_bytes(kThreads, kBatchRowLogE));
     smem_dec_tc_ = dec_tc_smem_bytes(std::max(kmax_tc, 1));
     smem_crt_ = crt_smem_bytes(kmax);
     smem_crt_tc_ = crt_tc_smem_bytes(lw_tc);

@@ -11,6 +11,19 @@ namespace nc {
 
 enum : uint32_t { kItemDec = 0, kItemRow = 1, kItemCrt = 2 };
 
+// Row items of the persistent launch: radix 8 on the launch's 256-thread CTAs, row blocks of at
+// most 2^11 residues (one block per CTA at 2^11). Radix 16 on blocks of 2^12 took ~60% longer per
+// row at N = 2^16 and needs twice the registers for its sixteen values.
+constexpr int kBatchRowLogE = 3;
+constexpr int kBatchRowLogMax = 11;
+inline RowConfig batch_row_config(int logN) {
+    RowConfig c{};
+    c.logN2 = logN < kBatchRowLogMax ? logN : kBatchRowLogMax;
+    c.logE = kBatchRowLogE;
+    c.threads = kThreads;
+    return c;
+}
+
 // One product of a batch with the item counts its dependents wait for.
 struct BatchProduct {
     ProductDesc d;

@@ -68,9 +68,9 @@ __device__ __forceinline__ void batch_item(uint32_t stage, const BatchProduct& b
     } else if (stage == kItemRow) {
         switch (bp.d.logN2) {
 #define NC_B_ROW(n) \
-    case n: row_blocks<n, 4, kThreads>(bp.d, t, idx, smem); break;
+    case n: row_blocks<n, kBatchRowLogE, kThreads>(bp.d, t, idx, smem); break;
             NC_B_ROW(1) NC_B_ROW(2) NC_B_ROW(3) NC_B_ROW(4) NC_B_ROW(5) NC_B_ROW(6)
-            NC_B_ROW(7) NC_B_ROW(8) NC_B_ROW(9) NC_B_ROW(10) NC_B_ROW(11) NC_B_ROW(12)
+            NC_B_ROW(7) NC_B_ROW(8) NC_B_ROW(9) NC_B_ROW(10) NC_B_ROW(11)
 #undef NC_B_ROW
             default: break;
         }
@@ -165,7 +165,7 @@ cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
     cudaError_t e = upload_prime_constants(pc, pow32);
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smax(dec_smem_bytes(kMaxPrimes), row_smem_bytes(kThreads, 4))));
+                             int(smax(dec_smem_bytes(kMaxPrimes), row_smem_bytes(kThreads, kBatchRowLogE))));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_batch_crt, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(crt_smem_bytes(kMaxPrimes)));
