@@ -218,7 +218,8 @@ void Batch::finalize(cudaStream_t stream) {
     smem_crt_ = crt_smem_bytes(kmax);
     smem_crt_tc_ = crt_tc_smem_bytes(lw_tc);
     int per_sm = 0, sms = 0;
-    check(persistent_occupancy(smem_, &per_sm), "occupancy");
+    with_dec_ = !dec.empty();
+    check(persistent_occupancy(smem_, with_dec_, &per_sm), "occupancy");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "device attribute");
     ctas_ = std::max(1, std::min(per_sm * sms, n_items_));
     if (shape != shape_) {
@@ -270,7 +271,7 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
             e = launch_batch_dec_tc(dt, l, smem_dec_tc_, s);
             at += n_dec_tc_[l];
         }
-        if (e == cudaSuccess && n_items_ > 0) e = launch_persistent(args, ctas_, smem_, s);
+        if (e == cudaSuccess && n_items_ > 0) e = launch_persistent(args, ctas_, smem_, s, with_dec_);
         if (e == cudaSuccess && n_crt_tc_ > 0) e = launch_batch_crt(tc, true, smem_crt_tc_, s);
         if (e == cudaSuccess && n_crt_ > 0) e = launch_batch_crt(im, false, smem_crt_, s);
         if (!direct_.empty()) {

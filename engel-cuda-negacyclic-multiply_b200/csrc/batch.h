@@ -88,6 +88,7 @@ class Batch {
     int n_items_ = 0;
     int ctas_ = 0;
     size_t smem_ = 0;      // persistent launch (row items, and residue items on the integer pipes)
+    bool with_dec_ = false;  // the persistent queue holds residue items
     int n_crt_tc_ = 0;     // CRT items on the tensor cores, after the persistent queue in d_items_
     int n_crt_ = 0;        // CRT items on the integer pipes, after those
     size_t smem_crt_tc_ = 0, smem_crt_ = 0;

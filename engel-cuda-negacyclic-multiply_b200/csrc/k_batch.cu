@@ -55,9 +55,12 @@ __device__ __forceinline__ void batch_dec(const BatchProduct& bp, const Tables& 
     dec_tile<LW>(bp.d, t, operand, idx % int(bp.tiles), smem);
 }
 
+// WITH_DEC: the queue may hold residue items (products on the integer residue engine); without
+// them the kernel compiles the row items alone, with fewer registers and spills.
+template <bool WITH_DEC>
 __device__ __forceinline__ void batch_item(uint32_t stage, const BatchProduct& bp, const Tables& t, int idx,
                                            uint8_t* smem) {
-    if (stage == kItemDec) {
+    if (WITH_DEC && stage == kItemDec) {
         switch (bp.d.LW) {
 #define NC_B_DEC(n) \
     case n: batch_dec<n>(bp, t, idx, smem); break;
@@ -77,6 +80,7 @@ __device__ __forceinline__ void batch_item(uint32_t stage, const BatchProduct& b
     }
 }
 
+template <bool WITH_DEC>
 __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ int s_item;
@@ -97,7 +101,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
         }
         __syncthreads();
         if (s_go) {
-            batch_item(stage, bp, a.tables, int(w.y), smem);
+            batch_item<WITH_DEC>(stage, bp, a.tables, int(w.y), smem);
             __threadfence();
             __syncthreads();
             if (threadIdx.x == 0 && stage == kItemDec) atomicAdd(a.counters + 2 * prod, 1u);
@@ -164,8 +168,11 @@ cudaError_t launch_batch_crt(const BatchCrtArgs& args, bool tensor_cores, size_t
 cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
     cudaError_t e = upload_prime_constants(pc, pow32);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_persistent<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(smax(dec_smem_bytes(kMaxPrimes), row_smem_bytes(kThreads, kBatchRowLogE))));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_persistent<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(row_smem_bytes(kThreads, kBatchRowLogE)));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_batch_crt, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(crt_smem_bytes(kMaxPrimes)));
@@ -175,16 +182,18 @@ cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
     return e;
 }
 
-// Launch with `ctas` persistent CTAs and `smem` dynamic shared memory.
-cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s) {
+// Launch with `ctas` persistent CTAs and `smem` dynamic shared memory; `with_dec` when the queue
+// holds residue items.
+cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s, bool with_dec) {
     BatchArgs a = args;
     void* params[] = {&a};
-    return cudaLaunchKernel(reinterpret_cast<void*>(&k_persistent), dim3(unsigned(ctas)), dim3(kThreads), params,
-                            smem, s);
+    void* fn = with_dec ? reinterpret_cast<void*>(&k_persistent<true>) : reinterpret_cast<void*>(&k_persistent<false>);
+    return cudaLaunchKernel(fn, dim3(unsigned(ctas)), dim3(kThreads), params, smem, s);
 }
 
-cudaError_t persistent_occupancy(size_t smem, int* ctas_per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_persistent, kThreads, smem);
+cudaError_t persistent_occupancy(size_t smem, bool with_dec, int* ctas_per_sm) {
+    return with_dec ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_persistent<true>, kThreads, smem)
+                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_persistent<false>, kThreads, smem);
 }
 
 }  // namespace nc
