@@ -35,6 +35,10 @@ __device__ __forceinline__ uint64_t kmajor_desc(uint32_t addr, uint32_t lbo, uin
 
 constexpr uint32_t kMmaWaitLimit = 1u << 22;
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
 __device__ __forceinline__ bool mma_wait(uint32_t bar, uint32_t parity) {
     for (uint32_t it = 0; it < kMmaWaitLimit; ++it) {
         uint32_t done;
@@ -161,7 +165,9 @@ __device__ void crt_coeffs_tc(const ProductDesc& d, const Tables& t, int tile, u
         s_q[w] = __ldg(qc->q + w);
     }
     if (tid < 4) s_mu[tid] = __ldg(qc->mu + tid);
-    for (int w = tid; w < NC * 16; w += blockDim.x) reinterpret_cast<uint4*>(sB)[w] = __ldg(d.crt_b + w);
+    // the table is first read by the MMAs: its copy runs behind the column stages
+    for (int w = tid; w < NC * 16; w += blockDim.x) crt_tc_detail::cp_async16(sB + 16 * w, d.crt_b + w);
+    asm volatile("cp.async.commit_group;" ::: "memory");
     __syncthreads();
 
     switch (logN1) {
@@ -172,7 +178,8 @@ __device__ void crt_coeffs_tc(const ProductDesc& d, const Tables& t, int tile, u
         case 4: crt_tc_detail::crt_columns_tc<4>(d, t, j0, T, s_y, s_ys, s_p, sA); break;
         default: crt_tc_detail::crt_columns_tc<5>(d, t, j0, T, s_y, s_ys, s_p, sA); break;
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // A's generic stores -> MMA reads
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // A's and B's writes -> MMA reads
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -295,15 +302,18 @@ __device__ void crt_coeffs_tc(const ProductDesc& d, const Tables& t, int tile, u
     __syncthreads();
     const int N1 = 1 << logN1;
     const int seg = C * L;
-    for (int u = 0; u < N1; ++u) {
-        const size_t first = (size_t(u) * N2 + j0) * L;
-        uint32_t* dst = d.c + first;
-        const uint32_t* src = s_out + u * seg;
-        if (((first | size_t(seg)) & 3) == 0) {
-            uint4* d4 = reinterpret_cast<uint4*>(dst);
-            const uint4* s4 = reinterpret_cast<const uint4*>(src);
-            for (int w = tid; w < (seg >> 2); w += blockDim.x) d4[w] = s4[w];
-        } else {
+    if (((size_t(N2) * L | size_t(j0) * L | size_t(seg)) & 3) == 0) {
+        // every row segment starts on 16 bytes: one pass over all of them, every thread busy
+        const int seg4 = seg >> 2;
+        for (int w = tid; w < N1 * seg4; w += blockDim.x) {
+            const int u = w / seg4, x = w - u * seg4;
+            reinterpret_cast<uint4*>(d.c + (size_t(u) * N2 + j0) * L)[x] =
+                reinterpret_cast<const uint4*>(s_out + u * seg)[x];
+        }
+    } else {
+        for (int u = 0; u < N1; ++u) {
+            uint32_t* dst = d.c + (size_t(u) * N2 + j0) * L;
+            const uint32_t* src = s_out + u * seg;
             for (int w = tid; w < seg; w += blockDim.x) dst[w] = src[w];
         }
     }
