@@ -300,23 +300,7 @@ __device__ void crt_coeffs_tc(const ProductDesc& d, const Tables& t, int tile, u
         }
     }
     __syncthreads();
-    const int N1 = 1 << logN1;
-    const int seg = C * L;
-    if (((size_t(N2) * L | size_t(j0) * L | size_t(seg)) & 3) == 0) {
-        // every row segment starts on 16 bytes: one pass over all of them, every thread busy
-        const int seg4 = seg >> 2;
-        for (int w = tid; w < N1 * seg4; w += blockDim.x) {
-            const int u = w / seg4, x = w - u * seg4;
-            reinterpret_cast<uint4*>(d.c + (size_t(u) * N2 + j0) * L)[x] =
-                reinterpret_cast<const uint4*>(s_out + u * seg)[x];
-        }
-    } else {
-        for (int u = 0; u < N1; ++u) {
-            uint32_t* dst = d.c + (size_t(u) * N2 + j0) * L;
-            const uint32_t* src = s_out + u * seg;
-            for (int w = tid; w < seg; w += blockDim.x) dst[w] = src[w];
-        }
-    }
+    store_tile(d.c, N2, L, j0, C, 1 << logN1, s_out);
 }
 
 }  // namespace nc

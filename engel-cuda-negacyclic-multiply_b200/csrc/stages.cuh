@@ -39,21 +39,43 @@ static inline cudaError_t upload_prime_constants(const PrimeConst* pc, const uin
 // ------------------------------------------------------------------------------------------
 // stage 1: residues + forward column stages
 
-// Loads the CTA's tile (N1 segments of C consecutive coefficients) into shared memory.
+// Loads the CTA's tile (N1 segments of C consecutive coefficients) into shared memory. When
+// every segment starts on 16 bytes, one pass over all segments' 16-byte chunks keeps every
+// thread busy (a pass per segment left most of them idle for short segments).
 __device__ __forceinline__ void load_tile(const uint32_t* x, int N2, int L, int j0, int C, int N1,
                                           uint32_t* s_in) {
     const int seg = C * L;
-    for (int u = 0; u < N1; ++u) {
-        const size_t first = (size_t(u) * N2 + j0) * L;
-        const uint32_t* src = x + first;
-        uint32_t* dst = s_in + u * seg;
-        if (((first | size_t(seg)) & 3) == 0) {
-            const uint4* s4 = reinterpret_cast<const uint4*>(src);
-            uint4* d4 = reinterpret_cast<uint4*>(dst);
-            for (int w = threadIdx.x; w < (seg >> 2); w += blockDim.x) d4[w] = __ldg(s4 + w);
-        } else {
-            for (int w = threadIdx.x; w < seg; w += blockDim.x) dst[w] = __ldg(src + w);
+    if (((size_t(N2) * L | size_t(j0) * L | size_t(seg)) & 3) == 0) {
+        const int seg4 = seg >> 2;
+        for (int w = threadIdx.x; w < N1 * seg4; w += blockDim.x) {
+            const int u = w / seg4, c = w - u * seg4;
+            reinterpret_cast<uint4*>(s_in + u * seg)[c] =
+                __ldg(reinterpret_cast<const uint4*>(x + (size_t(u) * N2 + j0) * L) + c);
         }
+        return;
+    }
+    for (int u = 0; u < N1; ++u) {
+        const uint32_t* src = x + (size_t(u) * N2 + j0) * L;
+        uint32_t* dst = s_in + u * seg;
+        for (int w = threadIdx.x; w < seg; w += blockDim.x) dst[w] = __ldg(src + w);
+    }
+}
+
+// The CTA's staged output tile (N1 segments of C coefficients in s_out) to its place in c.
+__device__ __forceinline__ void store_tile(uint32_t* c, int N2, int L, int j0, int C, int N1, const uint32_t* s_out) {
+    const int seg = C * L;
+    if (((size_t(N2) * L | size_t(j0) * L | size_t(seg)) & 3) == 0) {
+        const int seg4 = seg >> 2;
+        for (int w = threadIdx.x; w < N1 * seg4; w += blockDim.x) {
+            const int u = w / seg4, x = w - u * seg4;
+            reinterpret_cast<uint4*>(c + (size_t(u) * N2 + j0) * L)[x] = reinterpret_cast<const uint4*>(s_out + u * seg)[x];
+        }
+        return;
+    }
+    for (int u = 0; u < N1; ++u) {
+        uint32_t* dst = c + (size_t(u) * N2 + j0) * L;
+        const uint32_t* src = s_out + u * seg;
+        for (int w = threadIdx.x; w < seg; w += blockDim.x) dst[w] = src[w];
     }
 }
 
@@ -683,20 +705,7 @@ __device__ void crt_coeffs(const ProductDesc& d, const Tables& t, int tile, uint
         }
     }
     __syncthreads();
-    const int N1 = 1 << logN1;
-    const int seg = C * L;
-    for (int u = 0; u < N1; ++u) {
-        const size_t first = (size_t(u) * N2 + j0) * L;
-        uint32_t* dst = d.c + first;
-        const uint32_t* src = s_out + u * seg;
-        if (((first | size_t(seg)) & 3) == 0) {
-            uint4* d4 = reinterpret_cast<uint4*>(dst);
-            const uint4* s4 = reinterpret_cast<const uint4*>(src);
-            for (int w = threadIdx.x; w < (seg >> 2); w += blockDim.x) d4[w] = s4[w];
-        } else {
-            for (int w = threadIdx.x; w < seg; w += blockDim.x) dst[w] = src[w];
-        }
-    }
+    store_tile(d.c, N2, L, j0, C, 1 << logN1, s_out);
 }
 
 }  // namespace nc
