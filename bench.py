@@ -68,6 +68,22 @@ def parse_args():
     ap.add_argument("--row-config", type=str, default="",
                     help="pin the row configuration (log_block,log_radix,threads) instead of autotuning, e.g. to "
                          "profile the configuration a plain run picked")
+    pc = ap.add_argument_group("profiling modes (untimed runs for ncu; they print no bench line)")
+    pc.add_argument("--profile-case", action="store_true",
+                    help="run --profile-reps device-resident products of one seeded case and check the last one")
+    pc.add_argument("--profile-N", type=int, default=16384)
+    pc.add_argument("--profile-bits", type=int, default=868)
+    pc.add_argument("--profile-reps", type=int, default=3)
+    pc.add_argument("--profile-seed", type=int, default=7)
+    pc.add_argument("--profile-batch", type=int, default=0,
+                    help="each rep is one batch of this many products (persistent launch) instead of one product")
+    pc.add_argument("--profile-residue-engine", choices=["tc", "imad"], default="tc",
+                    help="residue stage of the products: k_dec_tc (tensor cores) or k_dec (integer pipes)")
+    pc.add_argument("--profile-residues", choices=["", "imad", "tc"], default="",
+                    help="run only the residue stage of both operands with this engine (k_residues_imad / "
+                         "k_residues_tc), checked against the other engine")
+    pc.add_argument("--profile-reference", type=int, default=0, metavar="PRODUCTS",
+                    help="run the reference's own binary on this many products of the bench workload")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.steps = max(a.steps, 1)
@@ -146,11 +162,17 @@ class ClockSampler:
 # ----------------------------------------------------------------------------- roofline
 
 
-def stage_work(k: int, N: int, L: int) -> list[float]:
+def stage_work(k: int, N: int, L: int, logN2: int | None = None) -> list[float]:
     """Algorithmic IMAD per stage: 8 per 64-bit mulmod, 2 per u32 x u64 limb MAC, 4 L per
-    coefficient for the final reduction. Whole product: 8 k N (1.5 log2 N + 7) + 6 k N L + 4 L N."""
+    coefficient for the final reduction. Whole product: 8 k N (1.5 log2 N + 7) + 6 k N L + 4 L N.
+    logN2 is the row block of the plan's row configuration (its row kernel runs logN2 stages of
+    each transform; the residue and CRT kernels run the other logN1 = log2 N - logN2 column
+    stages); the per-stage split depends on it, the product total does not."""
     logN = N.bit_length() - 1
-    logN2 = min(logN, 12)
+    if logN2 is None:
+        logN2 = min(logN, 12)
+    if not 0 <= logN2 <= logN:
+        raise ValueError("row block larger than the ring degree")
     logN1 = logN - logN2
     mm1 = 2 * k * N + 2 * k * N + 2 * k * (N // 2) * logN1   # residue reductions, twists, column stages
     mac1 = 2 * k * N * L
@@ -200,7 +222,7 @@ def run_harness(binary: Path, case, warmup: int, steps: int, timeout: float = 60
             raise RuntimeError(f"{binary.name}: {sum(row['status'] != 'ok' for row in rows)} cases failed")
         secs = [row["seconds"] for row in rows[warmup:]]
         out = cases.read_output(root, warmup + steps - 1, case.N, case.L)
-        return secs, res["init_s"], out
+        return secs, res["init_s"], out, rows[0]["seconds"]
 
 
 # ----------------------------------------------------------------------------- CPU baseline
@@ -355,7 +377,7 @@ def ours(args) -> dict | None:
     peak = nc.imad_peak()
     k, N, L = plan.k, case.N, case.L
     mean_stage = [statistics.mean(s[i] for s in stage) for i in range(3)]
-    work = stage_work(k, N, L)
+    work = stage_work(k, N, L, plan.row_config[0])
     sbytes = stage_bytes(k, N, L)
     dom = max(range(3), key=lambda i: mean_stage[i])
     crt_tc = plan.crt_engine == nc.CRT_TC_I8
@@ -394,6 +416,9 @@ def ours(args) -> dict | None:
             "unit": "GIMAD/s",
             "frac": achieved * 1e9 / peak,
             "traffic": traffic,
+            "frac_recomputed_from": ("stage_imad_alg[dom] / stage_ms[dom] / peak; the stage shares agree with the "
+                                     "ncu launch list in profiles/launches_bench_n65536.md, DRAM bytes in "
+                                     "profiles/traffic.json"),
             "peak_source": "measured live: mad.lo.u32 chains over every SM (nc_imad_peak)",
             "stage_ms": mean_stage,
             "stage_imad_alg": work,
@@ -411,15 +436,27 @@ def ours(args) -> dict | None:
     if rank == 0 and not args.no_e2e and RUNNER.exists():
         # about a millisecond per call: more calls than the device-timed steps, for a stable mean
         e2e_warmup, e2e_steps = max(args.warmup, 10), max(args.steps, 60)
-        secs, init_s, out = run_harness(RUNNER, case, e2e_warmup, e2e_steps)
+        secs, init_s, out, first_s = run_harness(RUNNER, case, e2e_warmup, e2e_steps)
         if not np.array_equal(out, ref):
             raise RuntimeError("harness runner output differs from the library")
         per = statistics.mean(secs)
+        h2d_gbs, d2h_gbs = copy_rates(dev, 2 * N * L * 4, N * L * 4)
+        h2d_ms = 2 * N * L * 4 / (h2d_gbs * 1e9) * 1e3
+        d2h_ms = N * L * 4 / (d2h_gbs * 1e9) * 1e3
         result["e2e"] = {"value": world / per, "unit": "products/s",
                          "h2d_bytes_per_step": 2 * N * L * 4, "d2h_bytes_per_step": N * L * 4,
                          "ms_p50": 1e3 * statistics.median(secs), "ms_p99": 1e3 * sorted(secs)[int(0.99 * (len(secs) - 1))],
+                         "first_call_ms": 1e3 * first_s,
+                         "floor_ms": h2d_ms + mean_stage[1] + d2h_ms,
+                         "floor": {"h2d_gbs": h2d_gbs, "d2h_gbs": d2h_gbs, "h2d_ms": h2d_ms, "row_stage_ms": mean_stage[1],
+                                   "d2h_ms": d2h_ms,
+                                   "why": ("every input byte crosses PCIe before the row stage can finish (each row "
+                                           "block needs residues of coefficients from the whole operand), and every "
+                                           "output byte after it; copy rates measured here from pinned memory in the "
+                                           "library's chunk sizes (4 MiB up, 2 MiB down), one direction at a time")},
                          "calls": e2e_steps, "warmup_calls": e2e_warmup, "init_s": init_s,
-                         "via": "fherma_run in the library's harness runner (pageable std::vector in/out)"}
+                         "via": "fherma_run in the library's harness runner (pageable std::vector in/out); "
+                                "first_call_ms is the first call after fherma_init"}
     if forms:
         # each form checks its own results; a failure is reported in its entry, not hidden
         for key, what, fn in (("batched_n65536", "batched N=65536", lambda: batched_same_shape(dev, case.q, 65536, 16, args)),
@@ -439,6 +476,38 @@ def ours(args) -> dict | None:
     if pg:
         pg.destroy_process_group()
     return result if rank == 0 else None
+
+
+def copy_rates(dev, up_bytes: int, down_bytes: int, reps: int = 5) -> tuple[float, float]:
+    """GB/s of pinned host -> device copies of `up_bytes` in 4 MiB chunks and device -> pinned host
+    copies of `down_bytes` in 2 MiB chunks (the host path's chunk sizes), best of `reps`."""
+    import torch
+
+    host = torch.empty(max(up_bytes, down_bytes), dtype=torch.uint8, pin_memory=True)
+    host.fill_(1)
+    devbuf = torch.empty_like(host, device=dev)
+    s = torch.cuda.current_stream(dev)
+
+    def timed(fn) -> float:
+        best = 1e30
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    def up():
+        for o in range(0, up_bytes, 4 << 20):
+            devbuf[o:min(up_bytes, o + (4 << 20))].copy_(host[o:min(up_bytes, o + (4 << 20))], non_blocking=True)
+
+    def down():
+        for o in range(0, down_bytes, 2 << 20):
+            host[o:min(down_bytes, o + (2 << 20))].copy_(devbuf[o:min(down_bytes, o + (2 << 20))], non_blocking=True)
+
+    return up_bytes / (timed(up) * 1e-3) / 1e9, down_bytes / (timed(down) * 1e-3) / 1e9
 
 
 # ----------------------------------------------------------------------------- batched forms
@@ -774,6 +843,24 @@ def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
     return out
 
 
+REF_KERNELS_FILE = ROOT / "profiles" / "reference_kernels_n65536.json"
+
+
+def _reference_device_time() -> dict | None:
+    """The reference's kernel time per product (sum of its launches' ncu durations over whole
+    products, from the committed launch-list summary), beside its wall-clock value."""
+    try:
+        tf = json.loads(REF_KERNELS_FILE.read_text())
+    except Exception:
+        return None
+    ms = tf.get("device_ms_per_product")
+    if not ms:
+        return None
+    return {"value": 1e3 / ms, "unit": "products/s", "ms_per_product": ms,
+            "source": f"{REF_KERNELS_FILE.relative_to(ROOT)} (ncu gpu__time_duration.sum per launch, "
+                      f"serialised and cold-cache)"}
+
+
 def _hbm_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     try:
@@ -789,15 +876,18 @@ def reference(args) -> dict | None:
     if rank != 0:
         return None
     case = cases.make_case(N_MAIN, BITS, SEED, edge_frac=EDGE)
+    N, L = case.N, case.L
     base = {"metric": METRIC, "unit": "products/s", "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u64", "data": "synthetic (seeded)", "config": config("reference, one process")}
+            "dtype": "u64", "data": "synthetic (seeded)", "config": config(f"replicas{world}")}
     why = None
     if REF_BINARY.exists():
         try:
-            secs, init_s, _ = run_harness(REF_BINARY, case, args.warmup, args.steps)
+            secs, init_s, _, first_s = run_harness(REF_BINARY, case, args.warmup, args.steps)
             per = statistics.mean(secs)
             v = 1.0 / per
+            # fherma_run of the reference copies both operands in and the product out inside the
+            # timed call (solve.cu:1499-1520), so its wall clock is an end-to-end figure
             base.update({"value": v, "ms_per_step": 1e3 * per, "init_s": init_s,
                          "cpu_baseline": {"value": v, "unit": "products/s", "cores": 1, "kind": "reference",
                                           "sample": f"reference solve.cu (sm_100a; kMaxN raised to 65536 and the "
@@ -805,8 +895,14 @@ def reference(args) -> dict | None:
                                                     f"with its own harness main.cpp, "
                                                     f"{args.steps} timed products after {args.warmup} warm-up; "
                                                     f"its kernels run on the GPU, one host thread drives them"},
-                         "e2e": {"value": v, "unit": "products/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                         "e2e": {"value": v, "unit": "products/s", "h2d_bytes_per_step": 2 * N * L * 4,
+                                 "d2h_bytes_per_step": N * L * 4, "ms_p50": 1e3 * statistics.median(secs),
+                                 "first_call_ms": 1e3 * first_s,
+                                 "via": "fherma_run in the reference's own harness main.cpp (wall clock)"},
                          "gpu_launches": None})
+            dev_ref = _reference_device_time()
+            if dev_ref:
+                base["device"] = dev_ref
             return base
         except Exception as e:  # fall back to the CPU oracle
             why = str(e)[:300]
@@ -817,8 +913,97 @@ def reference(args) -> dict | None:
     return base
 
 
+# ----------------------------------------------------------------------------- profiling modes
+
+
+def profile_case(a) -> int:
+    """Device-resident products of one seeded case for a profiler: each rep enqueues the three
+    kernels of one product (k_dec_tc or k_dec, k_row, k_crt_tc) on the default stream with the
+    --row-config configuration (default: the plan's default); with --profile-batch B each rep is
+    one batch of B products (k_persistent and the batched residue / CRT launches); with
+    --profile-residues each rep is the residue stage alone of both operands (k_residues_imad or
+    k_residues_tc). The run ends by checking the last result against the host entry point (or,
+    for --profile-residues, against the other residue engine)."""
+    import numpy as np
+    import torch
+
+    import cases
+    import negacyclic as nc
+
+    case = cases.make_case(a.profile_N, a.profile_bits, a.profile_seed, edge_frac=0.01)
+    dev = torch.device("cuda", 0)
+    da = torch.from_numpy(case.a.view(np.int32)).to(dev)
+    db = torch.from_numpy(case.b.view(np.int32)).to(dev)
+    if a.profile_residues:
+        engine = nc.RESIDUES_TC_I8 if a.profile_residues == "tc" else nc.RESIDUES_IMAD
+        other = nc.RESIDUES_IMAD if engine == nc.RESIDUES_TC_I8 else nc.RESIDUES_TC_I8
+        with nc.Plan(case.N, case.q_limbs, W=case.W) as plan:
+            k, N = plan.k, plan.N
+            r = torch.empty(2 * k * N, dtype=torch.int64, device=dev)
+            check = torch.empty_like(r)
+            for _ in range(a.profile_reps):
+                for j, x in enumerate((da, db)):
+                    plan.residues(x.data_ptr(), r.data_ptr() + j * k * N * 8, engine)
+            for j, x in enumerate((da, db)):
+                plan.residues(x.data_ptr(), check.data_ptr() + j * k * N * 8, other)
+            torch.cuda.synchronize()
+            ok = bool(torch.equal(r, check)) and not nc.residues_gave_up()
+        print(f"residues N={case.N} bits={a.profile_bits} reps={a.profile_reps} engine={a.profile_residues} "
+              f"consistent={ok}")
+        return 0 if ok else 1
+    count = max(1, a.profile_batch)
+    dcs = [torch.empty_like(da) for _ in range(count)]
+    with nc.Plan(case.N, case.q_limbs, W=case.W) as plan:
+        if a.row_config:
+            plan.row_config = tuple(int(x) for x in a.row_config.split(","))
+        if a.profile_residue_engine == "imad" or plan.k > 32:
+            plan.residue_engine = nc.RESIDUES_IMAD
+        if a.profile_batch > 0:
+            with nc.Batch() as batch:
+                for dc in dcs:
+                    batch.add(plan, da.data_ptr(), db.data_ptr(), dc.data_ptr())
+                for _ in range(a.profile_reps):
+                    batch.run(0, False)
+                batch.synchronize()
+        else:
+            for _ in range(a.profile_reps):
+                plan.multiply_device(da.data_ptr(), db.data_ptr(), dcs[0].data_ptr(), 0)
+        torch.cuda.synchronize()
+        want = plan.multiply(case.a, case.b)
+        cfg = plan.row_config
+    ok = all(np.array_equal(dc.cpu().numpy().view(np.uint32), want) for dc in dcs)
+    print(f"N={case.N} bits={a.profile_bits} reps={a.profile_reps} batch={a.profile_batch} config={cfg} consistent={ok}")
+    return 0 if ok else 1
+
+
+def profile_reference(a) -> int:
+    """The reference's own binary (its harness main.cpp) on `--profile-reference` products of the
+    bench workload, for a launch list of its kernels; its last product is checked against the
+    library's product of the same case."""
+    import numpy as np
+
+    import cases
+
+    case = cases.make_case(N_MAIN, BITS, SEED, edge_frac=EDGE)
+    if not REF_BINARY.exists():
+        print(f"no reference binary at {REF_BINARY.relative_to(ROOT)}")
+        return 1
+    _, _, out, _ = run_harness(REF_BINARY, case, 0, a.profile_reference)
+    import negacyclic as nc
+
+    with nc.Plan(case.N, case.q_limbs, W=case.W) as plan:
+        want = plan.multiply(case.a, case.b)
+    ok = bool(np.array_equal(out, want))
+    print(f"reference products={a.profile_reference} N={case.N} matches_library={ok}")
+    return 0 if ok else 1
+
+
 def main() -> int:
     args = parse_args()
+    if args.profile_case:
+        return profile_case(args)
+    if args.profile_reference:
+        return profile_reference(args)
     out = reference(args) if args.impl == "reference" else ours(args)
     if out is not None:
         print(json.dumps(out))

@@ -59,6 +59,26 @@ int nc_plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, nc_pla
     });
 }
 
+int nc_self_check(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
+    return guarded([&] {
+        if (N < 2 || N > uint32_t(nc::kMaxN) || (N & (N - 1)) != 0)
+            throw nc::Error(nc::kEInval, "N must be a power of two from 2 to 65536");
+        if (L == 0 || L > uint32_t(nc::kMaxL)) throw nc::Error(nc::kEInval, "L must be between 1 and 32");
+        if (!q) throw nc::Error(nc::kEInval, "q is null");
+        int logN = 0;
+        while ((1u << logN) < N) ++logN;
+        nc::QConst c{};
+        const std::string err = nc::build_qconst(q, int(L), logN, &c);
+        if (!err.empty()) throw nc::Error(nc::kEInval, err);
+        if (W != 0 && (W < c.qbits || (W + 31) / 32 != L))
+            throw nc::Error(nc::kEInval, "W must be the bit width of q and L = (W + 31) / 32");
+        const std::string& host = nc::host_self_check();
+        if (!host.empty()) throw nc::Error(nc::kESelfCheck, "init self-check: " + host);
+        const std::string qerr = nc::check_qconst(c);
+        if (!qerr.empty()) throw nc::Error(nc::kESelfCheck, "init self-check of the plan's constants: " + qerr);
+    });
+}
+
 int nc_plan_destroy(nc_plan* plan) {
     return guarded([&] {
         if (!plan) return;
@@ -119,6 +139,8 @@ int nc_plan_set_crt_engine(nc_plan* plan, int engine) {
         if (engine != NC_CRT_IMAD && engine != NC_CRT_TC_I8) throw nc::Error(nc::kEInval, "unknown CRT engine");
         if (engine == NC_CRT_TC_I8 && !plan->p->d_crt_b)
             throw nc::Error(nc::kEInval, "the tensor-core CRT takes at most 32 primes (q up to about 960 bits)");
+        if (engine == NC_CRT_TC_I8 && !plan->p->tables->tensor_cores)
+            throw nc::Error(nc::kEInval, "the tensor-core CRT needs a compute capability 10.0 device");
         plan->p->crt_tc = engine == NC_CRT_TC_I8;
     });
 }
@@ -135,6 +157,8 @@ int nc_plan_set_residue_engine(nc_plan* plan, int engine) {
     return guarded([&] {
         if (!plan) throw nc::Error(nc::kEInval, "null plan");
         if (engine != NC_RESIDUES_IMAD && engine != NC_RESIDUES_TC_I8) throw nc::Error(nc::kEInval, "unknown residue engine");
+        if (engine == NC_RESIDUES_TC_I8 && !plan->p->tables->tensor_cores)
+            throw nc::Error(nc::kEInval, "the tensor-core residue stage needs a compute capability 10.0 device");
         plan->p->res_tc = engine == NC_RESIDUES_TC_I8;
     });
 }

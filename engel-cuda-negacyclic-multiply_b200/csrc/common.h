@@ -18,6 +18,21 @@
 #define NC_HD
 #endif
 
+// Tensor-core (tcgen05) instructions exist only in the arch-specific sm_100a target. nvcc
+// -arch=sm_100a (the form a CMake project passes) also emits family-portable compute_100 PTX, in
+// which the tensor-core kernels compile to empty bodies: a B200 runs the sm_100a code, and
+// plan set-up keeps those kernels off any other device. NC_NO_TCGEN05 leaves them out of every
+// target (the single-file solve.cu build, whose link-time optimisation cannot take them); the
+// residue and CRT stages then run on the integer pipes.
+#if defined(NC_NO_TCGEN05)
+#define NC_HAS_TCGEN05 0
+#elif !defined(__CUDA_ARCH__) || defined(__CUDA_ARCH_FEAT_SM100_ALL) || defined(__CUDA_ARCH_SPECIFIC__) || \
+    defined(__CUDA_ARCH_FAMILY_SPECIFIC__)
+#define NC_HAS_TCGEN05 1
+#else
+#define NC_HAS_TCGEN05 0
+#endif
+
 namespace nc {
 
 constexpr int kMaxPrimes = 48;       // same residue budget as solve.cu:22 kMaxChannels

@@ -41,11 +41,15 @@ DeviceTables* acquire_tables(int device) {
         return it->second;
     }
     const HostTables& h = host_tables();
-    for (const auto& c : h.pc)
-        if (c.m >= (1ull << 28)) throw Error(kEInval, "internal: prime set outside the 2^62 - m, m < 2^28 shape");
+    const std::string& host_err = host_self_check();
+    if (!host_err.empty()) throw Error(kESelfCheck, "init self-check: " + host_err);
     auto* t = new DeviceTables();
     t->device = device;
     try {
+        int major = 0, minor = 0;
+        check(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "device attribute");
+        check(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device), "device attribute");
+        t->tensor_cores = NC_HAS_TCGEN05 && major == 10 && minor == 0;
         const size_t tw_bytes = size_t(kMaxPrimes) * kMaxN * sizeof(ulonglong2);
         check(cudaMalloc(&t->fwd, tw_bytes), "twiddle table");
         check(cudaMalloc(&t->inv, tw_bytes), "inverse twiddle table");
@@ -75,6 +79,7 @@ DeviceTables* acquire_tables(int device) {
         check(cudaMalloc(&t->res_w, w.size()), "residue weight table");
         check(cudaMemcpy(t->res_w, w.data(), w.size(), cudaMemcpyHostToDevice), "residue weight upload");
         check(prepare_kernels(h.pc.data(), h.pow32.data()), "kernel preparation");
+        check(prepare_noalloc(device), "allocation-free scratch set-up");
         // a synchronous copy from pageable memory may return before its last DMA lands, and the
         // kernels run on non-blocking streams that do not order after it: wait for the device
         check(cudaDeviceSynchronize(), "table upload");
@@ -107,6 +112,19 @@ void release_tables(DeviceTables* t) {
     cudaFree(t->res_w);
     cudaSetDevice(prev);
     delete t;
+}
+
+// Host-side self-checks, once per process: known answers of the host arithmetic, the prime set,
+// and a sample of every prime's tables (psi, 2^(32 l) mod p, twiddles and Shoup companions).
+const std::string& host_self_check() {
+    static std::string err;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        err = check_arithmetic();
+        if (err.empty()) err = check_prime_set();
+        if (err.empty()) err = check_tables(host_tables(), 64);
+    });
+    return err;
 }
 
 // ------------------------------------------------------------------------------ host pool
@@ -248,11 +266,17 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int fac
         delete p;
         throw Error(kEInval, "W must be the bit width of q and L = (W + 31) / 32");
     }
+    const std::string qerr = check_qconst(p->hq);
+    if (!qerr.empty()) {
+        delete p;
+        throw Error(kESelfCheck, "init self-check of the plan's constants: " + qerr);
+    }
     p->k = int(p->hq.k);
     if (!tuned_row_config(logN, int(L), &p->cfg)) p->cfg = default_row_config(logN);
     try {
         p->device = current_device();
         p->tables = acquire_tables(p->device);
+        if (!p->tables->tensor_cores) p->res_tc = p->crt_tc = false;  // integer-pipe engines only
         check(cudaMalloc(&p->d_qc, sizeof(QConst)), "plan constants");
         check(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking), "stream");
         // ordered on the plan's stream and complete before any other stream can use the plan
@@ -269,11 +293,80 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int fac
         check(cudaEventCreate(&p->ev_start), "event");
         check(cudaEventCreate(&p->ev_stop), "event");
         for (auto& ev : p->ev_stage) check(cudaEventCreate(&ev), "event");
+        device_self_test(p->device);
     } catch (...) {
         plan_destroy(p);
         throw;
     }
     return p;
+}
+
+namespace {
+std::mutex g_selftest_mu;
+std::map<int, int> g_selftest;  // device -> 1 while its self-test runs, 2 once it passed
+}  // namespace
+
+// Once per device, before the first plan there is handed out: an N = 8 product modulo
+// q = 2^127 - 1 with 0, 1 and q - 1 among its coefficients, by the default stages (tensor-core
+// residues and CRT where the device has them) and by the integer-pipe stages, compared with the
+// host schoolbook. The plan it creates runs no self-test of its own.
+void device_self_test(int device) {
+    {
+        std::lock_guard<std::mutex> lock(g_selftest_mu);
+        int& st = g_selftest[device];
+        if (st != 0) return;
+        st = 1;
+    }
+    constexpr int N = 8, L = 4;
+    const uint32_t q[L] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0x7fffffffu};
+    std::vector<uint32_t> a(N * L), b(N * L), want(N * L), got(N * L);
+    uint64_t x = 0x243f6a8885a308d3ull;
+    for (int i = 0; i < N * L; ++i) {
+        x = x * 6364136223846793005ull + 1442695040888963407ull;
+        a[size_t(i)] = uint32_t(x >> 32);
+        b[size_t(i)] = uint32_t(x >> 7);
+    }
+    for (int c = 0; c < N; ++c) {  // below q: top limbs under 2^31 - 1
+        a[size_t(c) * L + 3] &= 0x7ffffffeu;
+        b[size_t(c) * L + 3] &= 0x7ffffffeu;
+    }
+    for (int l = 0; l < L; ++l) {
+        a[size_t(1) * L + l] = q[l] - (l == 0 ? 1u : 0u);  // q - 1
+        b[size_t(2) * L + l] = q[l] - (l == 0 ? 1u : 0u);
+        a[size_t(3) * L + l] = 0;
+        b[size_t(5) * L + l] = l == 0 ? 1u : 0u;
+    }
+    schoolbook_negacyclic(N, L, q, a.data(), b.data(), want.data());
+    Plan* p = nullptr;
+    uint32_t* d = nullptr;
+    std::string err;
+    try {
+        p = plan_create(N, 0, L, q);
+        check(cudaMalloc(&d, size_t(3) * N * L * 4), "self-test buffers");
+        check(cudaMemcpy(d, a.data(), size_t(N) * L * 4, cudaMemcpyHostToDevice), "self-test upload");
+        check(cudaMemcpy(d + N * L, b.data(), size_t(N) * L * 4, cudaMemcpyHostToDevice), "self-test upload");
+        for (int engines = 0; engines < 2 && err.empty(); ++engines) {
+            if (engines == 1) p->res_tc = p->crt_tc = false;
+            check(cudaMemsetAsync(d + 2 * N * L, 0xff, size_t(N) * L * 4, p->stream), "self-test output");
+            plan_multiply_device(p, d, d + N * L, d + 2 * N * L, p->stream);
+            check(cudaStreamSynchronize(p->stream), "self-test product");
+            check(cudaMemcpy(got.data(), d + 2 * N * L, size_t(N) * L * 4, cudaMemcpyDeviceToHost), "self-test download");
+            if (got != want)
+                err = engines == 0 ? "the default stages' N = 8 product differs from the schoolbook"
+                                   : "the integer-pipe stages' N = 8 product differs from the schoolbook";
+        }
+    } catch (...) {
+        cudaFree(d);
+        plan_destroy(p);
+        std::lock_guard<std::mutex> lock(g_selftest_mu);
+        g_selftest[device] = 0;
+        throw;
+    }
+    cudaFree(d);
+    plan_destroy(p);
+    std::lock_guard<std::mutex> lock(g_selftest_mu);
+    g_selftest[device] = err.empty() ? 2 : 0;
+    if (!err.empty()) throw Error(kESelfCheck, "device self-test: " + err);
 }
 
 // The plain path's residue scratch (2 k N u64), allocated on its first use: plans used only

@@ -23,7 +23,7 @@ struct Error : std::runtime_error {
     Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
-enum : int { kOk = 0, kEInval = -1, kECuda = -2, kENoMem = -3, kETimeout = -4, kEBusy = -5 };
+enum : int { kOk = 0, kEInval = -1, kECuda = -2, kENoMem = -3, kETimeout = -4, kEBusy = -5, kESelfCheck = -6 };
 
 void check(cudaError_t e, const char* what);
 
@@ -37,8 +37,17 @@ struct DeviceTables {
     uint64_t* pow32 = nullptr;   // [kMaxPrimes][kMaxL]
     uint64_t* primes = nullptr;  // [kMaxPrimes]
     uint4* res_w = nullptr;      // weight bytes of the tensor-core residue stage
+    bool tensor_cores = false;   // compute capability 10.0: the sm_100a tcgen05 kernels run here
     Tables view() const { return Tables{fwd, inv, pow32, primes, res_w}; }
 };
+
+// Known answers of the host arithmetic, the prime set and sampled tables, checked once per
+// process ("" when they hold).
+const std::string& host_self_check();
+
+// An N = 8 product on `device` against the host schoolbook, once per device (the first plan
+// created there runs it); throws Error(kESelfCheck) on a mismatch.
+void device_self_test(int device);
 
 DeviceTables* acquire_tables(int device);
 void release_tables(DeviceTables* t);

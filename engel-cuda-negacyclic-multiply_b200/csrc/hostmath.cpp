@@ -154,6 +154,40 @@ Big divmod(Big a, const Big& m, Big* quot) {
     return a;
 }
 
+Big add_big(const Big& a, const Big& b) {
+    Big r(std::max(a.size(), b.size()) + 1, 0);
+    uint64_t carry = 0;
+    for (size_t i = 0; i + 1 < r.size(); ++i) {
+        const uint64_t cur = uint64_t(i < a.size() ? a[i] : 0) + (i < b.size() ? b[i] : 0) + carry;
+        r[i] = uint32_t(cur);
+        carry = cur >> 32;
+    }
+    r.back() = uint32_t(carry);
+    trim(r);
+    return r;
+}
+
+Big mul_big(const Big& a, const Big& b) {
+    Big r(a.size() + b.size() + 1, 0);
+    for (size_t i = 0; i < a.size(); ++i) {
+        uint64_t carry = 0;
+        for (size_t j = 0; j < b.size(); ++j) {
+            const uint64_t cur = uint64_t(r[i + j]) + uint64_t(a[i]) * b[j] + carry;
+            r[i + j] = uint32_t(cur);
+            carry = cur >> 32;
+        }
+        for (size_t t = i + b.size(); carry; ++t) {
+            const uint64_t cur = uint64_t(r[t]) + carry;
+            r[t] = uint32_t(cur);
+            carry = cur >> 32;
+        }
+    }
+    trim(r);
+    return r;
+}
+
+int cmp_big(const Big& a, const Big& b) { return cmp_shifted(a, b, 0); }
+
 Big pow2(int e) {
     Big r(size_t(e / 32 + 1), 0);
     r[e / 32] = 1u << (e % 32);
@@ -252,6 +286,122 @@ const HostTables& host_tables() {
         for (auto& th : pool) th.join();
     });
     return t;
+}
+
+// ---------------------------------------------------------------------------- self-checks
+
+std::string check_arithmetic() {
+    // the reference's fherma_init opens with known answers of its modular helpers
+    // (solve.cu:1151-1165); these are the same facts for the helpers used here
+    if (mulmod64(7, 5, 11) != 2) return "mulmod64(7, 5, 11) != 2";
+    if (powmod64(3, 10, 11) != 1) return "powmod64(3, 10, 11) != 1";
+    if (uint64_t((u128(1) << 64) / 3) != 6148914691236517205ull || uint64_t((u128(1) << 64) % 3) != 1)
+        return "2^64 / 3 division";
+    if (!is_prime64(2305843009213693951ull) || is_prime64(2305843009213693953ull)) return "Miller-Rabin on 2^61 - 1";
+    const Big q{0xffffffffu, 0xffffffffu, 0xffffffffu, 0x7fffffffu};  // 2^127 - 1
+    const Big x = mul_big(q, q);
+    Big quo;
+    const Big r = divmod(add_big(x, Big{5}), q, &quo);
+    if (r != Big{5} || quo != q) return "big-integer (2^127 - 1)^2 + 5 division";
+    return std::string();
+}
+
+std::string check_prime_set() {
+    const auto& ps = prime_set();
+    if (int(ps.size()) != kMaxPrimes) return "prime set size";
+    for (int i = 0; i < kMaxPrimes; ++i) {
+        const PrimeConst& c = ps[size_t(i)];
+        if (!is_prime64(c.p)) return "prime " + std::to_string(i) + " is composite";
+        if (((c.p - 1) & ((1ull << kRootLog) - 1)) != 0) return "prime " + std::to_string(i) + " is not 1 mod 2^17";
+        if (c.m != (1ull << 62) - c.p || c.m >= (1ull << 28)) return "prime " + std::to_string(i) + " is not 2^62 - m";
+        if (u128(c.g) * c.p > (u128(1) << 93) || (u128(c.g) + 1) * c.p <= (u128(1) << 93))
+            return "prime " + std::to_string(i) + ": g != floor(2^93 / p)";
+        if (i > 0 && c.p >= ps[size_t(i) - 1].p) return "prime set not descending";
+    }
+    return std::string();
+}
+
+std::string check_tables(const HostTables& t, int samples) {
+    for (int i = 0; i < kMaxPrimes; ++i) {
+        const uint64_t p = t.pc[size_t(i)].p;
+        const uint64_t psi = t.psi[size_t(i)];
+        const std::string at = "prime " + std::to_string(i) + ": ";
+        if (powmod64(psi, 1ull << kMaxLogN, p) != p - 1) return at + "psi^(2^16) != -1";
+        for (int l = 0; l < kMaxL; ++l)
+            if (t.pow32[size_t(i) * kMaxL + size_t(l)] != powmod64(2, 32ull * uint64_t(l), p))
+                return at + "2^(32 l) mod p";
+        const uint64_t* f = t.fwd.data() + size_t(i) * kMaxN * 2;
+        const uint64_t* g = t.inv.data() + size_t(i) * kMaxN * 2;
+        for (int s = 0; s < samples; ++s) {
+            const uint32_t j = uint32_t((uint64_t(s) * 2654435761u + uint64_t(i)) % uint64_t(kMaxN));
+            const uint32_t e = bitrev(j, kMaxLogN);
+            if (f[2 * j] != powmod64(psi, e, p)) return at + "twiddle psi^bitrev(j)";
+            if (mulmod64(f[2 * j], g[2 * j], p) != 1) return at + "inverse twiddle";
+            for (const uint64_t* w : {f + 2 * j, g + 2 * j}) {
+                const u128 lhs = u128(w[0]) << 64, qp = u128(w[1]) * p;  // w' = floor(w 2^64 / p)
+                if (qp > lhs || lhs - qp >= p) return at + "Shoup companion of a twiddle";
+            }
+        }
+    }
+    return std::string();
+}
+
+std::string check_qconst(const QConst& c) {
+    const int k = int(c.k), L = int(c.L);
+    const auto& ps = prime_set();
+    if (k < 1 || k > kMaxPrimes || L < 1 || L > kMaxL) return "prime or limb count";
+    Big qb(c.q, c.q + L);
+    trim(qb);
+    if (bits_of(qb) != int(c.qbits)) return "bit length of q";
+    Big neg(c.neg_m, c.neg_m + kMqStride);
+    trim(neg);
+    if (cmp_big(neg, qb) >= 0) return "(-M) mod q is not below q";
+    const uint64_t N = 1ull << c.logN;
+    for (int i = 0; i < k; ++i) {
+        const uint64_t p = ps[size_t(i)].p;
+        const std::string at = "prime " + std::to_string(i) + ": ";
+        // y_i (M / p_i) N = 1 (mod p_i), with M / p_i mod p_i formed as a product of the other primes
+        uint64_t mi = 1;
+        for (int j = 0; j < k; ++j)
+            if (j != i) mi = mulmod64(mi, ps[size_t(j)].p % p, p);
+        if (mulmod64(mulmod64(c.y[i], mi, p), N % p, p) != 1) return at + "y_i (M/p_i) N != 1 mod p_i";
+        const u128 lhs = u128(c.y[i]) << 64, qp = u128(c.ys[i]) * p;
+        if (qp > lhs || lhs - qp >= p) return at + "Shoup companion of y_i";
+        // (M / p_i mod q) p_i + ((-M) mod q) = 0 (mod q)
+        Big mq(c.mq + size_t(i) * kMqStride, c.mq + size_t(i) * kMqStride + kMqStride);
+        trim(mq);
+        if (cmp_big(mq, qb) >= 0) return at + "(M/p_i) mod q is not below q";
+        if (!divmod(add_big(mul_u64(mq, p), neg), qb, nullptr).empty()) return at + "(M/p_i mod q) p_i != M mod q";
+    }
+    // mu = floor(2^(qbits + kBarrettT + 1) / q): mu q <= 2^e < (mu + 1) q
+    Big mu(c.mu, c.mu + 4);
+    trim(mu);
+    const Big e = pow2(int(c.qbits) + kBarrettT + 1);
+    if (cmp_big(mul_big(mu, qb), e) > 0 || cmp_big(add_big(mul_big(mu, qb), qb), e) <= 0) return "Barrett constant mu";
+    return std::string();
+}
+
+void schoolbook_negacyclic(int N, int L, const uint32_t* q, const uint32_t* a, const uint32_t* b, uint32_t* c) {
+    Big qb(q, q + L);
+    trim(qb);
+    for (int k = 0; k < N; ++k) {
+        Big pos, neg;
+        for (int i = 0; i < N; ++i) {
+            const int j = k - i >= 0 ? k - i : k - i + N;
+            Big x(a + size_t(i) * L, a + size_t(i) * L + L), y(b + size_t(j) * L, b + size_t(j) * L + L);
+            trim(x);
+            trim(y);
+            if (k - i >= 0)
+                pos = add_big(pos, mul_big(x, y));
+            else
+                neg = add_big(neg, mul_big(x, y));
+        }
+        pos = divmod(pos, qb, nullptr);
+        neg = divmod(neg, qb, nullptr);
+        if (cmp_big(pos, neg) < 0) pos = add_big(pos, qb);
+        if (!neg.empty()) sub_shifted(pos, neg, 0);
+        for (int l = 0; l < L; ++l) c[size_t(k) * L + size_t(l)] = size_t(l) < pos.size() ? pos[size_t(l)] : 0;
+    }
 }
 
 std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out, int factors) {

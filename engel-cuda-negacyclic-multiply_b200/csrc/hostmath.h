@@ -37,6 +37,18 @@ int primes_needed(int logN, int qbits, int factors = 2);
 // Fill the CRT + Barrett constants. Returns an empty string or an error message.
 std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out, int factors = 2);
 
+// Self-checks run before a plan is handed out, as the reference's fherma_init checks its
+// arithmetic before it returns a state (solve.cu:1151-1165, 1285-1314, 1370-1415); unlike its
+// L = 28 Barrett check, these hold for every valid q. Each returns "" or what failed.
+std::string check_arithmetic();                              // known answers of the host helpers
+std::string check_prime_set();                               // primes, their 2^62 - m form, floor(2^93 / p)
+std::string check_tables(const HostTables& t, int samples);  // psi, 2^(32 l) mod p, sampled twiddles
+std::string check_qconst(const QConst& c);                   // CRT identities and mu of one plan
+
+// c = a * b mod (X^N + 1, q) by the schoolbook sum on big integers (small N only: the device
+// self-test's expected answer).
+void schoolbook_negacyclic(int N, int L, const uint32_t* q, const uint32_t* a, const uint32_t* b, uint32_t* c);
+
 // Small helpers shared with the tests of the host math.
 uint64_t mulmod64(uint64_t a, uint64_t b, uint64_t p);
 uint64_t powmod64(uint64_t a, uint64_t e, uint64_t p);

@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_crt(BatchCrtArgs a) {
 }
 
 __global__ void __launch_bounds__(kThreads, 2) k_batch_crt_tc(BatchCrtArgs a) {
+#if NC_HAS_TCGEN05
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
@@ -156,6 +157,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_crt_tc(BatchCrtArgs a) {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(taddr) : "memory");
+#endif
 }
 
 cudaError_t launch_batch_crt(const BatchCrtArgs& args, bool tensor_cores, size_t smem, cudaStream_t s) {

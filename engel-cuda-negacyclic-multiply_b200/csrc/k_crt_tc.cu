@@ -6,6 +6,7 @@ namespace nc {
 
 template <int LW>
 __global__ void __launch_bounds__(kThreads, 2) k_crt_tc(ProductDesc d, Tables t) {
+#if NC_HAS_TCGEN05
     constexpr uint32_t kCols = crt_tc_tmem_cols(LW);
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
@@ -30,6 +31,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_crt_tc(ProductDesc d, Tables t)
     __syncthreads();
     if (threadIdx.x < 32)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kCols) : "memory");
+#endif
 }
 
 void* crt_tc_kernel(int LW) {

@@ -268,16 +268,19 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
 // Plain path: one product, grid = operands x tiles.
 template <int LOG_N1>
 __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_dec_tc(ProductDesc d, Tables t, int first_operand, int tiles) {
+#if NC_HAS_TCGEN05
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
     dec_tc_item<LOG_N1>(d, t, first_operand + int(blockIdx.x) / tiles, int(blockIdx.x) % tiles, smem, bar, taddr_slot);
+#endif
 }
 
 // Batches: one CTA per item (x = product, y = operand * tiles + tile), every product of the launch
 // with the same column length N1.
 template <int LOG_N1>
 __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_batch_dec_tc(BatchCrtArgs a) {
+#if NC_HAS_TCGEN05
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
@@ -286,6 +289,7 @@ __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_batch_dec_tc(BatchCrtArgs a) {
     const int tiles = int(bp.tiles_tc);
     dec_tc_item<LOG_N1>(bp.d, a.tables, int(bp.first_operand) + int(w.y) / tiles, int(w.y) % tiles, smem, bar,
                         taddr_slot);
+#endif
 }
 
 void* batch_dec_tc_kernel(int logN1) {

@@ -30,6 +30,7 @@
 #include "hostmath.h"
 #include "kernel_registry.h"
 #include "negacyclic_b200.h"
+#include "crt_tc.cuh"
 #include "stages.cuh"
 
 namespace nc {
@@ -96,13 +97,8 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Shared-memory matrix descriptor for a K-major operand without swizzling: 8-row x 16-byte core
-// matrices, `lbo` bytes between the two K-adjacent core matrices of one MMA, `sbo` bytes between
-// row groups of 8; descriptor version 1 (bits 46-47), layout type 0 (no swizzle).
-__device__ __forceinline__ uint64_t kmajor_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
-           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
-}
+// Shared-memory matrix descriptor of a K-major operand without swizzling (crt_tc.cuh).
+using crt_tc_detail::kmajor_desc;
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     for (uint32_t it = 0; it < kTcSpinLimit; ++it) {
@@ -129,6 +125,7 @@ __device__ __forceinline__ void add128(uint64_t& lo, uint64_t& hi, uint64_t add_
 // [8 rows][16 B], B (weight bytes) as [prime][K chunk 8][8 byte planes][16 B], the MMA's mbarrier
 // and the tensor-memory address slot.
 __global__ void __launch_bounds__(128) k_residues_tc(TcArgs a) {
+#if NC_HAS_TCGEN05
     extern __shared__ __align__(16) uint8_t tc_smem[];  // core matrices need 16-byte alignment
     uint8_t* sA = tc_smem;
     uint8_t* sB = tc_smem + kTcRows * kTcKBytes;
@@ -223,6 +220,7 @@ __global__ void __launch_bounds__(128) k_residues_tc(TcArgs a) {
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(a.tmem_cols) : "memory");
+#endif
 }
 
 // Per device: the weight table (kMaxPrimes x kTcGroupBytes) and the status word.
@@ -293,6 +291,7 @@ void residues(const Plan* p, const uint32_t* d_x, uint64_t* d_r, int engine, cud
     }
     if (engine != NC_RESIDUES_TC_I8) throw Error(kEInval, "unknown residue engine");
     if (p->k > kTcMaxGroups) throw Error(kEInval, "the tensor-core engine takes at most 32 primes (q up to ~960 bits)");
+    if (!p->tables->tensor_cores) throw Error(kEInval, "the tensor-core engine needs a compute capability 10.0 device");
     const TcDevice dev = tc_device(device);
     TcArgs a{};
     a.x = d_x;

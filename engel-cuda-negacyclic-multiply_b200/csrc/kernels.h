@@ -34,6 +34,10 @@ cudaError_t launch_residues(const ProductDesc& d, const Tables& t, const RowConf
 cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s,
                            cudaEvent_t* stage_events = nullptr, cudaEvent_t b_ready = nullptr);
 
+// Per device, with that device current: look up (and so load onto the device) the fixed scratch
+// array of the allocation-free entry point. Called once when the device's tables are set up.
+cudaError_t prepare_noalloc(int device);
+
 // Measured 32-bit IMAD throughput of this device (ops/s), from a mad.lo.u32 chain kernel.
 cudaError_t measure_imad_peak(double* ops_per_second);
 

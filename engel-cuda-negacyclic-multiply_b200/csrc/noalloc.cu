@@ -18,9 +18,12 @@
 // before the next stage reads it), but calls that overlap on the GPU race on it: order them on
 // one stream or synchronise between them.
 //
-// Set-up: host code cannot use the array's name as a device address, so the first call on a
-// device (with that device current) looks its address up with cudaGetSymbolAddress and keeps it;
-// that first call should come before any stream capture on the device.
+// Set-up: host code cannot use the array's name as a device address. When the library first
+// sets a device up (the first plan created on it uploads the device tables, with that device
+// current), prepare_noalloc looks the array's address up with cudaGetSymbolAddress, checks the
+// result and keeps it. That lookup is also what loads this file's module, and with it the array,
+// onto the device under CUDA's lazy module loading: so the allocation happens at plan creation,
+// and a call of the entry point never allocates or loads anything, not even its first.
 #include <cuda_runtime.h>
 
 #include <map>
@@ -43,11 +46,9 @@ std::map<int, uint64_t*> g_addr;  // device -> device address of g_static_residu
 uint64_t* static_residues(int device) {
     std::lock_guard<std::mutex> lock(g_addr_mu);
     auto it = g_addr.find(device);
-    if (it != g_addr.end()) return it->second;
-    void* ptr = nullptr;
-    check(cudaGetSymbolAddress(&ptr, g_static_residues), "static residue scratch address");
-    g_addr[device] = static_cast<uint64_t*>(ptr);
-    return static_cast<uint64_t*>(ptr);
+    if (it == g_addr.end())
+        throw Error(kEInval, "the allocation-free scratch was not set up on this device (create a plan on it first)");
+    return it->second;
 }
 
 void multiply_noalloc(const Plan* p, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t stream) {
@@ -72,6 +73,17 @@ void multiply_noalloc(const Plan* p, const uint32_t* d_a, const uint32_t* d_b, u
 }
 
 }  // namespace
+
+cudaError_t prepare_noalloc(int device) {
+    std::lock_guard<std::mutex> lock(g_addr_mu);
+    if (g_addr.count(device)) return cudaSuccess;
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_residues);
+    if (e != cudaSuccess) return e;
+    g_addr[device] = static_cast<uint64_t*>(ptr);
+    return cudaSuccess;
+}
+
 }  // namespace nc
 
 extern "C" int nc_multiply_device_noalloc(const nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,

@@ -167,6 +167,7 @@ void Server::release_operand(int id) {
     std::lock_guard<std::mutex> lock(mu_);
     auto it = operands_.find(id);
     if (it == operands_.end()) throw Error(kEInval, "unknown operand");
+    if (it->second.pins > 0) throw Error(kEBusy, "the operand is used by a request being submitted");
     for (auto& kv : requests_)
         if (kv.second->operand == id && kv.second->status < 2 && kv.second->status >= 0)
             throw Error(kEBusy, "the operand is used by a pending request");
@@ -182,28 +183,44 @@ uint64_t Server::submit(Plan* plan, const uint32_t* a, int operand, const uint32
     r->operand = operand;
     r->limb_bytes = granules(plan->limbs() * 4);
     r->dev_bytes = 3 * r->limb_bytes + 2 * granules(size_t(plan->k) * plan->N * 8);
+    auto check_operand = [&]() -> std::map<int, Operand>::iterator {
+        auto it = operands_.find(operand);
+        if (it == operands_.end()) throw Error(kEInval, "unknown operand");
+        if (it->second.plan->N != plan->N || it->second.plan->k != plan->k ||
+            std::memcmp(it->second.plan->hq.q, plan->hq.q, sizeof(plan->hq.q)) != 0)
+            throw Error(kEInval, "the operand was registered for another N or q");
+        return it;
+    };
     {
         std::unique_lock<std::mutex> lock(mu_);
         if (!fault_.empty()) throw Error(kECuda, "server stopped after a device error: " + fault_);
-        if (operand >= 0) {
-            auto it = operands_.find(operand);
-            if (it == operands_.end()) throw Error(kEInval, "unknown operand");
-            if (it->second.plan->N != plan->N || it->second.plan->k != plan->k ||
-                std::memcmp(it->second.plan->hq.q, plan->hq.q, sizeof(plan->hq.q)) != 0)
-                throw Error(kEInval, "the operand was registered for another N or q");
-        } else if (!a) {
+        if (operand >= 0)
+            check_operand();
+        else if (!a)
             throw Error(kEInval, "null operand a");
-        }
         if (3 * r->limb_bytes > host_arena_.capacity() || r->dev_bytes > dev_arena_.capacity())
             throw Error(kENoMem, "the request is larger than the server's budgets");
         space_cv_.wait(lock, [&] { return (r->host = host_arena_.alloc(3 * r->limb_bytes)) != nullptr || stop_; });
         if (stop_) throw Error(kEBusy, "server is stopping");
+        if (operand >= 0) {
+            // the lock is dropped for the staging copies below: pin the operand so that
+            // release_operand cannot free it before the request is queued (the wait above may
+            // also have let a release through, so the operand is looked up again here)
+            auto it = operands_.find(operand);
+            if (it == operands_.end()) {
+                host_arena_.free(r->host);
+                space_cv_.notify_all();
+                throw Error(kEInval, "unknown operand");
+            }
+            ++it->second.pins;
+        }
         r->id = next_id_++;
     }
     const size_t bytes = plan->limbs() * 4;
     if (operand < 0) stage_copy(r->host, reinterpret_cast<const char*>(a), bytes);
     stage_copy(r->host + r->limb_bytes, reinterpret_cast<const char*>(b), bytes);
     std::lock_guard<std::mutex> lock(mu_);
+    if (operand >= 0) --operands_.at(operand).pins;  // from here the queued request keeps it
     r->t_submit = now_ms();
     if (t_first_ < 0) t_first_ = r->t_submit;
     const uint64_t id = r->id;
@@ -284,32 +301,55 @@ void Server::launch(std::vector<Request*>& reqs) {
     cudaStream_t st = streams_[size_t(s)];
     Batch& batch = *batches_[size_t(s)];
     batch.clear();
+    // A request whose cached operand is gone (it cannot be: submit pins it and release_operand
+    // refuses operands of queued requests) fails on its own instead of reading a null operand.
+    std::vector<Request*> run;
     for (Request* r : reqs) {
-        const size_t bytes = r->plan->limbs() * 4;
-        char* da = r->dev;
-        char* db = r->dev + r->limb_bytes;
-        char* dc = r->dev + 2 * r->limb_bytes;
-        uint64_t* scratch = reinterpret_cast<uint64_t*>(r->dev + 3 * r->limb_bytes);
-        if (r->operand < 0) check(cudaMemcpyAsync(da, r->host, bytes, cudaMemcpyHostToDevice, st), "operand copy");
-        check(cudaMemcpyAsync(db, r->host + r->limb_bytes, bytes, cudaMemcpyHostToDevice, st), "operand copy");
-        if (r->operand >= 0)
-            batch.add(r->plan, kModeCachedA, nullptr, reinterpret_cast<uint32_t*>(db), reinterpret_cast<uint32_t*>(dc),
-                      reinterpret_cast<const uint64_t*>(operands_[r->operand].dev), nullptr, scratch);
-        else
-            batch.add(r->plan, kModeProduct, reinterpret_cast<uint32_t*>(da), reinterpret_cast<uint32_t*>(db),
-                      reinterpret_cast<uint32_t*>(dc), nullptr, nullptr, scratch);
-        r->status = 1;
+        if (r->operand >= 0 && operands_.find(r->operand) == operands_.end()) {
+            dev_arena_.free(r->dev);
+            r->dev = nullptr;
+            r->status = -1;
+            continue;
+        }
+        run.push_back(r);
     }
-    batch.run(st, false);
-    for (Request* r : reqs)
-        check(cudaMemcpyAsync(r->host + 2 * r->limb_bytes, r->dev + 2 * r->limb_bytes, r->plan->limbs() * 4,
-                              cudaMemcpyDeviceToHost, st),
-              "product copy");
+    if (run.size() != reqs.size()) done_cv_.notify_all();
+    reqs.swap(run);
+    if (reqs.empty()) return;
     Flight f;
-    f.reqs = reqs;
-    f.stream = s;
-    check(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming), "event");
-    check(cudaEventRecord(f.done, st), "event");
+    try {
+        for (Request* r : reqs) {
+            const size_t bytes = r->plan->limbs() * 4;
+            char* da = r->dev;
+            char* db = r->dev + r->limb_bytes;
+            char* dc = r->dev + 2 * r->limb_bytes;
+            uint64_t* scratch = reinterpret_cast<uint64_t*>(r->dev + 3 * r->limb_bytes);
+            if (r->operand < 0) check(cudaMemcpyAsync(da, r->host, bytes, cudaMemcpyHostToDevice, st), "operand copy");
+            check(cudaMemcpyAsync(db, r->host + r->limb_bytes, bytes, cudaMemcpyHostToDevice, st), "operand copy");
+            if (r->operand >= 0)
+                batch.add(r->plan, kModeCachedA, nullptr, reinterpret_cast<uint32_t*>(db),
+                          reinterpret_cast<uint32_t*>(dc),
+                          reinterpret_cast<const uint64_t*>(operands_.at(r->operand).dev), nullptr, scratch);
+            else
+                batch.add(r->plan, kModeProduct, reinterpret_cast<uint32_t*>(da), reinterpret_cast<uint32_t*>(db),
+                          reinterpret_cast<uint32_t*>(dc), nullptr, nullptr, scratch);
+            r->status = 1;
+        }
+        batch.run(st, false);
+        for (Request* r : reqs)
+            check(cudaMemcpyAsync(r->host + 2 * r->limb_bytes, r->dev + 2 * r->limb_bytes, r->plan->limbs() * 4,
+                                  cudaMemcpyDeviceToHost, st),
+                  "product copy");
+        f.reqs = reqs;
+        f.stream = s;
+        check(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming), "event");
+        check(cudaEventRecord(f.done, st), "event");
+    } catch (...) {
+        // copies or kernels of this batch may already be queued: the caller frees the requests'
+        // device blocks, so wait until nothing on the stream can still touch them
+        cudaStreamSynchronize(st);
+        throw;
+    }
     stream_busy_[size_t(s)] = true;
     flights_.push_back(std::move(f));
     ++batches_run_;

@@ -71,6 +71,7 @@ class Server {
         Plan* plan;
         char* dev;
         size_t bytes;
+        int pins = 0;  // submits between their operand check and their enqueue
     };
     struct Flight {
         std::vector<Request*> reqs;

@@ -19,7 +19,7 @@ import numpy as np
 PKG_DIR = Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "lib" / "libnegacyclic_b200.so"
 
-NC_OK, NC_EINVAL, NC_ECUDA, NC_ENOMEM, NC_ETIMEOUT, NC_EBUSY = 0, -1, -2, -3, -4, -5
+NC_OK, NC_EINVAL, NC_ECUDA, NC_ENOMEM, NC_ETIMEOUT, NC_EBUSY, NC_ESELFCHECK = 0, -1, -2, -3, -4, -5, -6
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
@@ -30,6 +30,7 @@ C_SYMBOLS = [
     ("nc_last_error", ctypes.c_char_p, []),
     ("nc_version", ctypes.c_int, []),
     ("nc_plan_create", ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.POINTER(_vp)]),
+    ("nc_self_check", ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p]),
     ("nc_plan_destroy", ctypes.c_int, [_vp]),
     ("nc_multiply", ctypes.c_int, [_vp, _u32p, _u32p, _u32p]),
     ("nc_multiply_device", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
@@ -127,6 +128,13 @@ def primes(count: int = 48) -> list[int]:
     out = (ctypes.c_uint64 * count)()
     _check(load().nc_primes(out, count))
     return list(out)
+
+
+def self_check(N: int, q_limbs: np.ndarray, W: int = 0) -> None:
+    """The init-time checks of plan creation that need no device (nc_self_check); raises
+    NegacyclicError (NC_EINVAL for an invalid point, NC_ESELFCHECK for a failed check)."""
+    q = np.ascontiguousarray(q_limbs, dtype=np.uint32)
+    _check(load().nc_self_check(N, W, len(q), _u32(q)))
 
 
 RESIDUES_IMAD, RESIDUES_TC_I8 = 0, 1

@@ -26,7 +26,9 @@ enum {
     NC_ECUDA = -2,    /* a CUDA call failed */
     NC_ENOMEM = -3,   /* device or pinned allocation failed, or an HBM budget is exceeded */
     NC_ETIMEOUT = -4, /* a persistent-kernel dependency wait gave up (bounded spin) */
-    NC_EBUSY = -5     /* the object is in use (server full, request not finished) */
+    NC_EBUSY = -5,    /* the object is in use (server full, request not finished) */
+    NC_ESELFCHECK = -6 /* an init-time self-check failed (host arithmetic, tables, plan constants,
+                          or the device's known-answer product) */
 };
 
 typedef struct nc_plan nc_plan;
@@ -44,6 +46,17 @@ int nc_version(void);
    the platform states it (L = (W + 31) / 32), or 0 to take it from q. Not reentrant: one
    product at a time per plan. */
 int nc_plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, nc_plan** out);
+
+/* The init-time checks of nc_plan_create that need no device, for one (N, q): known answers of
+   the host arithmetic, the prime set and a sample of every prime's tables (once per process), then
+   the plan's CRT constants: y_i (M/p_i) N = 1 mod p_i from an independent product of the other
+   primes, (M/p_i mod q) p_i + ((-M) mod q) = 0 mod q for every i, the Barrett constant's defining
+   inequality, and the Shoup companions. They hold for every valid q. Returns NC_OK, NC_EINVAL for
+   an invalid point, or NC_ESELFCHECK. nc_plan_create runs the same checks and, once per device,
+   an N = 8 known-answer product on the device. Mirrors the self-checks of the reference's
+   fherma_init (solve.cu:1151-1165, 1285-1314, 1370-1415), without its L = 28 Barrett check,
+   which rejects nearly every 868-bit q. */
+int nc_self_check(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q);
 
 /* Releases the plan (null is a no-op). Replaces fherma_free (fherma.h:47, solve.cu:1530-1567). */
 int nc_plan_destroy(nc_plan* plan);
@@ -63,8 +76,9 @@ int nc_multiply_device(nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, 
    (held on every GPU that loads it until exit) instead of the plan's own scratch. Limit:
    k * N <= 2^19 (N <= 16384 at an 868-bit q); larger products return NC_EINVAL. All calls share
    that array, so calls that overlap on the GPU race; nothing in it needs to start at zero. The
-   first call on a device looks up the array's device address and should come before any stream
-   capture on that device. This entry point has no counterpart in the reference. */
+   array's device address is looked up (and the array loaded onto the device) when the first plan
+   on that device is created, so no call of this entry point allocates, its first included. This
+   entry point has no counterpart in the reference. */
 int nc_multiply_device_noalloc(const nc_plan* plan, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
                                void* stream);
 

@@ -1,6 +1,6 @@
 """Generate tests/golden/reference_outputs.json from the reference's own binaries.
 
-    python tests/golden/make_golden.py --out gpurun_out/golden   # on a machine with a B200
+    python tests/golden/make_golden.py [--out DIR]   # on a machine with a B200 (default: tests/golden)
 
 For every seeded case below it writes a case directory in the platform's format, runs the
 reference solution built from its unmodified sources (oracle/_ref/solution) or, where that
@@ -69,7 +69,7 @@ def run_binary(binary: Path, c: cases.Case) -> tuple[str, bytes | None, str]:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=str(ROOT / "gpurun_out" / "golden"))
+    ap.add_argument("--out", default=str(Path(__file__).resolve().parent))
     a = ap.parse_args()
     out = Path(a.out)
     out.mkdir(parents=True, exist_ok=True)

@@ -152,3 +152,49 @@ def test_high_rate_overlapping_batches(gpu, mix):
     assert st["timeouts"] == 0
     assert not errors, errors[:5]
     assert st["completed"] == 320
+
+
+def test_release_operand_races_submit(gpu, mix):
+    """release_operand racing submits that name the operand: each release either is refused with
+    NC_EBUSY (a request still uses the operand) or succeeds, after which submits naming it fail
+    cleanly with NC_EINVAL; every request that was accepted returns the exact product."""
+    plans, _ = mix
+    p, q, L, reused = plans[0]  # N = 2^10: short requests, many interleavings
+    want = p.multiply(reused[0], reused[1])
+    for attempt in range(4):
+        with nc.Server(hbm_budget=1 << 28, staging=1 << 26, max_batch=8, streams=2) as srv:
+            op = srv.register_operand(p, reused[0])
+            accepted, refused, released = [], [], []
+
+            def submitter():
+                for _ in range(20):  # 60 requests in all: their staging fits at once
+                    try:
+                        accepted.append(srv.submit(p, None, reused[1], operand=op))
+                    except nc.NegacyclicError as e:
+                        refused.append(e.code)
+                        return
+
+            def releaser():
+                time.sleep(0.0005 * (attempt + 1))
+                while True:
+                    try:
+                        srv.release_operand(op)
+                        released.append(True)
+                        return
+                    except nc.NegacyclicError as e:
+                        if e.code != nc.NC_EBUSY:
+                            released.append(e.code)
+                            return
+                        time.sleep(0.0001)
+
+            subs = [threading.Thread(target=submitter) for _ in range(3)]
+            rel = threading.Thread(target=releaser)
+            for t in subs + [rel]:
+                t.start()
+            for t in subs + [rel]:
+                t.join(timeout=60)
+            assert released == [True]
+            assert all(code == nc.NC_EINVAL for code in refused), refused
+            for rid in accepted:
+                c, _ = srv.wait(rid, p)
+                assert np.array_equal(c, want)

@@ -1,0 +1,40 @@
+"""Init-time self-checks (nc_self_check; nc_plan_create runs the same ones, plus a device
+known-answer product). The reference's fherma_init checks its arithmetic before it returns a
+state (solve.cu:1151-1165, 1285-1314, 1370-1415), but its L = 28 Barrett check rejects nearly
+every 868-bit q; these must hold for every valid point, and reject invalid ones with a message."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import cases
+import negacyclic as nc
+
+
+@pytest.mark.parametrize("bits", [20, 62, 100, 434, 600, 868, 960, 1000, 1024])
+@pytest.mark.parametrize("log_n", [1, 4, 10, 14, 16])
+def test_self_check_holds_for_valid_points(bits, log_n):
+    q = cases.gen_prime(bits, 9000 + bits)
+    L = (bits + 31) // 32
+    nc.self_check(1 << log_n, cases.limbs_of(q, L), W=bits)
+
+
+def test_self_check_holds_for_composite_odd_moduli():
+    # the CRT and Barrett constants need q odd, not prime
+    for q in (3 ** 500, (1 << 867) + 1, (1 << 1023) + (1 << 500) + 1):
+        bits = q.bit_length()
+        nc.self_check(65536, cases.limbs_of(q, (bits + 31) // 32))
+
+
+@pytest.mark.parametrize("N,limbs,W,msg", [
+    (3, [7], 0, "power of two"),
+    (131072, [7], 0, "power of two"),
+    (1024, [8], 0, "odd"),
+    (1024, [7, 0], 0, "top limb"),
+    (1024, [7], 40, "bit width"),
+    (1024, [0xffffffff] * 33, 0, "L must be"),
+])
+def test_self_check_rejects_invalid_points(N, limbs, W, msg):
+    with pytest.raises(nc.NegacyclicError, match=msg) as ei:
+        nc.self_check(N, np.array(limbs, dtype=np.uint32), W=W)
+    assert ei.value.code == nc.NC_EINVAL

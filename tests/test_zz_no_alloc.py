@@ -42,6 +42,29 @@ def test_noalloc_matches_plan_scratch_on_two_calls(gpu, N, bits):
             assert torch.equal(got, want), f"call {call}: allocation-free product differs"
 
 
+def test_noalloc_calls_leave_device_memory_unchanged(gpu):
+    """No call allocates device memory, the first one on a fresh plan included: the fixed array
+    is placed on the device when the first plan there is created, not when the entry point runs."""
+    import torch
+
+    N, bits = 8192, 868
+    q = cases.gen_prime(bits, 4300)
+    L = (bits + 31) // 32
+    with nc.Plan(N, cases.limbs_of(q, L)) as plan:
+        a = _dev(cases.coeffs(q, N, L, 4301), gpu)
+        b = _dev(cases.coeffs(q, N, L, 4302), gpu)
+        want, got = torch.zeros_like(a), torch.full_like(a, -1)
+        # the plan-scratch path first: it loads the product kernels and allocates its own scratch
+        plan.multiply_device(a.data_ptr(), b.data_ptr(), want.data_ptr(), 0)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        for _ in range(2):
+            plan.multiply_device_noalloc(a.data_ptr(), b.data_ptr(), got.data_ptr(), 0)
+            torch.cuda.synchronize()
+            assert torch.cuda.mem_get_info()[0] == free_before, "an allocation-free call changed free device memory"
+        assert torch.equal(got, want)
+
+
 def test_noalloc_rejects_products_beyond_the_static_scratch(gpu):
     import torch
 
