@@ -817,12 +817,19 @@ def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
                 for th in threads:
                     th.join()
                 st = srv.stats()
+                io = srv.io_stats()
             if wrong or failed:
                 raise RuntimeError(f"served products differ from the plain path for plans {sorted(set(wrong))[:8]}; "
                                    f"{len(failed)} requests failed: {failed[:2]}")
+            win = io["device_window_ms"] * 1e-3
             row["server"] = {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": max(lat_srv),
                              "products_per_s": st["products_per_s"], "batches": st["batches"],
-                             "timeouts": st["timeouts"], "verified": len(lat_srv)}
+                             "timeouts": st["timeouts"], "verified": len(lat_srv),
+                             "h2d_gbs": io["h2d_bytes"] / win / 1e9 if win else None,
+                             "d2h_gbs": io["d2h_bytes"] / win / 1e9 if win else None,
+                             "device_busy_frac": io["device_busy_ms"] / io["device_window_ms"]
+                             if io["device_window_ms"] else None,
+                             "batch_size_mean": len(lat_srv) / st["batches"] if st["batches"] else None}
             # plain per-call form on the same schedule: one worker, host operands in and out
             lat = []
             t0 = time.perf_counter()

@@ -17,6 +17,16 @@ constexpr uint64_t kMask62 = (1ull << 62) - 1;
 
 __device__ __forceinline__ uint64_t csub(uint64_t x, uint64_t m) { return x >= m ? x - m : x; }
 
+// Programmatic dependent launch. A product kernel launched with it may be scheduled while the
+// kernel before it on the stream still runs (once every CTA of that kernel has called
+// pdl_trigger(), which each product kernel does on entry), so its prologue (tensor-memory
+// allocation, constant tables) overlaps that kernel's last wave. pdl_wait() returns once the
+// kernel before has completed and its writes are visible; every read or write of data that
+// kernel produces or consumes comes after it. In a kernel launched without the attribute, both
+// return at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // y * w mod p in [0, 2p) for any y < 2^64 and w < p, with wq = floor(w * 2^64 / p).
 __device__ __forceinline__ uint64_t shoup_lazy(uint64_t y, uint64_t w, uint64_t wq, uint64_t p) {
     const uint64_t q = __umul64hi(y, wq);

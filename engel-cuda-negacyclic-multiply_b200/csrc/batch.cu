@@ -110,6 +110,7 @@ void Batch::finalize(cudaStream_t stream) {
         scratch_bytes_ = scratch;
     }
     std::vector<uint2> dec, row, crt, crt_tc, dec_tc[kMaxLogN1 + 1];
+    std::vector<uint2> row_by_size[kBatchRowLogMax + 1];
     direct_.clear();
     int lw_tc = 2;
     size_t off = 0;
@@ -159,7 +160,10 @@ void Batch::finalize(cudaStream_t stream) {
         }
         bp.n_row = uint32_t(g.row_ctas);
         for (uint32_t i = 0; i < bp.n_dec; ++i) dec.push_back(make_uint2((kItemDec << 28) | pid, i));
-        for (uint32_t i = 0; i < bp.n_row; ++i) row.push_back(make_uint2((kItemRow << 28) | pid, i));
+        for (uint32_t i = 0; i < bp.n_row; ++i) {
+            row.push_back(make_uint2((kItemRow << 28) | pid, i));
+            row_by_size[cfg.logN2].push_back(make_uint2((kItemRow << 28) | pid, i));
+        }
         if (e.mode != kModeForward) {
             // CRT on the tensor cores for products with a table and at most 30 limbs
             const bool tc = d.crt_b && crt_tc_tmem_cols(int(d.LW)) == 256;
@@ -168,11 +172,23 @@ void Batch::finalize(cudaStream_t stream) {
         }
         shape.push_back((uint64_t(pl->logN) << 40) | (uint64_t(pl->k) << 32) | (uint64_t(pl->L) << 8) | e.mode);
     }
-    // queue of the persistent launch (residue, then row items), then the two CRT item lists
+    // queue of the persistent launch (residue, then row items; without residue items, the row
+    // items grouped by row-block size, one launch per group), then the two CRT item lists
+    with_dec_ = !dec.empty();
     std::vector<uint2> items;
     items.reserve(dec.size() + row.size() + crt_tc.size() + crt.size());
-    items.insert(items.end(), dec.begin(), dec.end());
-    items.insert(items.end(), row.begin(), row.end());
+    row_groups_.clear();
+    if (with_dec_) {
+        items.insert(items.end(), dec.begin(), dec.end());
+        items.insert(items.end(), row.begin(), row.end());
+    } else {
+        for (int l = kBatchRowLogMax; l >= 1; --l) {
+            if (row_by_size[l].empty()) continue;
+            row_groups_.push_back(RowGroup{l, int(items.size()), int(row_by_size[l].size()), 0});
+            items.insert(items.end(), row_by_size[l].begin(), row_by_size[l].end());
+            shape.push_back((uint64_t(3) << 60) | (uint64_t(l) << 32) | uint64_t(row_by_size[l].size()));
+        }
+    }
     n_items_ = int(items.size());
     n_crt_tc_ = int(crt_tc.size());
     n_crt_ = int(crt.size());
@@ -188,7 +204,7 @@ void Batch::finalize(cudaStream_t stream) {
 
     ensure(reinterpret_cast<char**>(&d_products_), &products_cap_, n * sizeof(BatchProduct), "batch products");
     ensure(&d_items_, &items_cap_, items.size(), "batch items");
-    ensure(&d_state_, &state_cap_, 2 * n + 5, "batch counters");
+    ensure(&d_state_, &state_cap_, 2 * n + 5 + kBatchRowLogMax, "batch counters");
     // Stream-ordered upload from pinned memory: the kernel on `stream` sees the tables only after
     // the copies (a synchronous copy from pageable memory may return before its DMA lands, and
     // nothing would order it before a launch on a non-blocking stream). The previous run has
@@ -218,10 +234,18 @@ void Batch::finalize(cudaStream_t stream) {
     smem_crt_ = crt_smem_bytes(kmax);
     smem_crt_tc_ = crt_tc_smem_bytes(lw_tc);
     int per_sm = 0, sms = 0;
-    with_dec_ = !dec.empty();
-    check(persistent_occupancy(smem_, with_dec_, &per_sm), "occupancy");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "device attribute");
-    ctas_ = std::max(1, std::min(per_sm * sms, n_items_));
+    if (with_dec_) {
+        check(persistent_occupancy(smem_, &per_sm), "occupancy");
+        ctas_ = std::max(1, std::min(per_sm * sms, n_items_));
+    } else {
+        ctas_ = 0;
+        for (RowGroup& g : row_groups_) {
+            check(persistent_rows_occupancy(g.logN2, &per_sm), "occupancy");
+            g.ctas = std::max(1, std::min(per_sm * sms, g.count));
+            ctas_ = std::max(ctas_, g.ctas);
+        }
+    }
     if (shape != shape_) {
         if (exec_) cudaGraphExecDestroy(exec_);
         if (graph_) cudaGraphDestroy(graph_);
@@ -271,7 +295,17 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
             e = launch_batch_dec_tc(dt, l, smem_dec_tc_, s);
             at += n_dec_tc_[l];
         }
-        if (e == cudaSuccess && n_items_ > 0) e = launch_persistent(args, ctas_, smem_, s, with_dec_);
+        if (with_dec_) {
+            if (e == cudaSuccess && n_items_ > 0) e = launch_persistent(args, ctas_, smem_, s);
+        } else {
+            for (size_t g = 0; g < row_groups_.size() && e == cudaSuccess; ++g) {
+                BatchArgs ga = args;
+                ga.items = d_items_ + row_groups_[g].first;
+                ga.n_items = row_groups_[g].count;
+                ga.head = d_state_ + 2 * n + 5 + g;
+                e = launch_persistent_rows(ga, row_groups_[g].logN2, row_groups_[g].ctas, s);
+            }
+        }
         if (e == cudaSuccess && n_crt_tc_ > 0) e = launch_batch_crt(tc, true, smem_crt_tc_, s);
         if (e == cudaSuccess && n_crt_ > 0) e = launch_batch_crt(im, false, smem_crt_, s);
         if (!direct_.empty()) {
@@ -282,7 +316,7 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
         }
         return e;
     };
-    const size_t state_bytes = (2 * n + 5) * sizeof(uint32_t);
+    const size_t state_bytes = (2 * n + 5 + kBatchRowLogMax) * sizeof(uint32_t);
     if (!use_graph) {
         check(cudaMemsetAsync(d_state_, 0, state_bytes, stream), "batch reset");
         check(enqueue(stream), "batch launch");

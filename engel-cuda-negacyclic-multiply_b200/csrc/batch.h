@@ -40,7 +40,8 @@ class Batch {
     int ctas() const { return ctas_; }
     size_t scratch_bytes() const { return scratch_bytes_; }
     int launches_per_run() const {
-        int n = (n_items_ > 0 ? 1 : 0) + (n_crt_tc_ > 0 ? 1 : 0) + (n_crt_ > 0 ? 1 : 0);
+        int n = (n_items_ > 0 ? (with_dec_ ? 1 : int(row_groups_.size())) : 0) + (n_crt_tc_ > 0 ? 1 : 0) +
+                (n_crt_ > 0 ? 1 : 0);
         for (int c : n_dec_tc_) n += c > 0 ? 1 : 0;
         for (const Direct& x : direct_) n += x.d.mode == kModeForward ? 2 : 3;
         return n;
@@ -67,6 +68,12 @@ class Batch {
         RowConfig cfg;
     };
     static constexpr int kDirectLogN = 15;
+    // Without residue items in the queue, the row items go by row-block size, one persistent
+    // launch each (k_persistent_rows<logN2>): items [first, first + count) of the queue.
+    struct RowGroup {
+        int logN2, first, count, ctas;
+    };
+    std::vector<RowGroup> row_groups_;
     void finalize(cudaStream_t stream);
     int device_;
     std::vector<Direct> direct_;
@@ -79,7 +86,7 @@ class Batch {
     size_t products_cap_ = 0;
     uint2* d_items_ = nullptr;
     size_t items_cap_ = 0;
-    uint32_t* d_state_ = nullptr;  // counters (2 per product), head, error
+    uint32_t* d_state_ = nullptr;  // counters (2 per product), head, error[4], a head per row group
     size_t state_cap_ = 0;
     char* h_upload_ = nullptr;  // pinned: product table | item list, copied on the run's stream
     size_t h_upload_cap_ = 0;

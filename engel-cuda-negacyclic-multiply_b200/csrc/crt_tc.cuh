@@ -169,6 +169,7 @@ __device__ void crt_coeffs_tc(const ProductDesc& d, const Tables& t, int tile, u
     for (int w = tid; w < NC * 16; w += blockDim.x) crt_tc_detail::cp_async16(sB + 16 * w, d.crt_b + w);
     asm volatile("cp.async.commit_group;" ::: "memory");
     __syncthreads();
+    pdl_wait();  // the residues come from the stream's previous kernel
 
     switch (logN1) {
         case 0: crt_tc_detail::crt_columns_tc<0>(d, t, j0, T, s_y, s_ys, s_p, sA); break;

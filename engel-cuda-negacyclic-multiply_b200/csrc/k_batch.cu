@@ -1,9 +1,11 @@
 // Batched kernels: the row stage of every product of a batch (and the residue stage of products on
-// the integer residue engine) in one persistent launch, then the CRT stage of every product in one
+// the integer residue engine) in persistent launches, then the CRT stage of every product in one
 // launch per CRT engine. Residues on the tensor cores run before, in k_batch_dec_tc (k_dec_tc.cu);
-// products of N >= 2^15 take the plain path's launches instead (batch.cu).
+// products of N >= 2^15 take the plain path's launches instead (batch.cu). When every residue is
+// made on the tensor cores, the row items run in one k_persistent_rows<logN2> launch per row-block
+// size present (no waits); otherwise k_persistent runs every residue and row item.
 //
-// Persistent launch: the host lays out a work queue of items (stage, product, index): all residue
+// k_persistent: the host lays out a work queue of items (stage, product, index): all residue
 // items of every product, then all row items. CTAs (as many as fit on the GPU at once) take items
 // in queue order with one atomic. A row item of product p may start once every residue item of p
 // is done; the CTA's first thread polls p's counter. Every item a CTA waits for was taken earlier
@@ -55,12 +57,10 @@ __device__ __forceinline__ void batch_dec(const BatchProduct& bp, const Tables& 
     dec_tile<LW>(bp.d, t, operand, idx % int(bp.tiles), smem);
 }
 
-// WITH_DEC: the queue may hold residue items (products on the integer residue engine); without
-// them the kernel compiles the row items alone, with fewer registers and spills.
-template <bool WITH_DEC>
+// A residue item (a product on the integer residue engine) or a row item of any row-block size.
 __device__ __forceinline__ void batch_item(uint32_t stage, const BatchProduct& bp, const Tables& t, int idx,
                                            uint8_t* smem) {
-    if (WITH_DEC && stage == kItemDec) {
+    if (stage == kItemDec) {
         switch (bp.d.LW) {
 #define NC_B_DEC(n) \
     case n: batch_dec<n>(bp, t, idx, smem); break;
@@ -80,11 +80,16 @@ __device__ __forceinline__ void batch_item(uint32_t stage, const BatchProduct& b
     }
 }
 
-template <bool WITH_DEC>
+// Queues with residue items (products on the integer residue engine): residue items, then row
+// items of any row-block size. The item's product descriptor is copied into shared memory once per
+// item, and the stages read its fields from there.
 __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ int s_item;
     __shared__ int s_go;
+    __shared__ __align__(16) BatchProduct s_bp;
+    constexpr int kWords = int(sizeof(BatchProduct) / 4);
+    static_assert(sizeof(BatchProduct) % 4 == 0, "descriptor copied in words");
     for (;;) {
         if (threadIdx.x == 0) s_item = int(atomicAdd(a.head, 1u));
         __syncthreads();
@@ -93,20 +98,58 @@ __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
         const uint2 w = __ldg(a.items + it);
         const uint32_t stage = w.x >> 28;
         const uint32_t prod = w.x & 0x0fffffffu;
-        const BatchProduct bp = a.products[prod];
+        if (threadIdx.x < kWords)
+            reinterpret_cast<uint32_t*>(&s_bp)[threadIdx.x] =
+                __ldg(reinterpret_cast<const uint32_t*>(a.products + prod) + threadIdx.x);
         if (threadIdx.x == 0) {
             bool ok = true;
-            if (stage == kItemRow) ok = wait_count(a.counters + 2 * prod, bp.n_dec, a.error, w.x);
+            if (stage == kItemRow) ok = wait_count(a.counters + 2 * prod, __ldg(&a.products[prod].n_dec), a.error, w.x);
             s_go = ok ? 1 : 0;
         }
         __syncthreads();
         if (s_go) {
-            batch_item<WITH_DEC>(stage, bp, a.tables, int(w.y), smem);
+            batch_item(stage, s_bp, a.tables, int(w.y), smem);
             __threadfence();
             __syncthreads();
             if (threadIdx.x == 0 && stage == kItemDec) atomicAdd(a.counters + 2 * prod, 1u);
         }
         __syncthreads();  // s_item / s_go are rewritten by the next round
+    }
+}
+
+// Row items alone, every one of them with row blocks of 2^LOG_N2 residues (the batch launches one
+// of these per row-block size present, after the residue launches): no item waits, and one
+// instantiation per kernel keeps the row stage at 80 registers without spills, three CTAs per SM
+// (the switch over every size in k_persistent<false> spills about 1.2 KB a thread).
+template <int LOG_N2>
+__global__ void __launch_bounds__(kThreads, 3) k_persistent_rows(BatchArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ int s_item;
+    __shared__ __align__(16) BatchProduct s_bp;
+    constexpr int kWords = int(sizeof(BatchProduct) / 4);
+    for (;;) {
+        if (threadIdx.x == 0) s_item = int(atomicAdd(a.head, 1u));
+        __syncthreads();
+        const int it = s_item;
+        if (it >= a.n_items) break;
+        const uint2 w = __ldg(a.items + it);
+        if (threadIdx.x < kWords)
+            reinterpret_cast<uint32_t*>(&s_bp)[threadIdx.x] =
+                __ldg(reinterpret_cast<const uint32_t*>(a.products + (w.x & 0x0fffffffu)) + threadIdx.x);
+        __syncthreads();
+        row_blocks<LOG_N2, kBatchRowLogE, kThreads>(s_bp.d, a.tables, int(w.y), smem);
+        __syncthreads();  // s_item and s_bp are rewritten by the next round
+    }
+}
+
+static void* persistent_rows_kernel(int logN2) {
+    switch (logN2) {
+#define NC_P_ROWS(n) \
+    case n: return reinterpret_cast<void*>(&k_persistent_rows<n>);
+        NC_P_ROWS(1) NC_P_ROWS(2) NC_P_ROWS(3) NC_P_ROWS(4) NC_P_ROWS(5) NC_P_ROWS(6)
+        NC_P_ROWS(7) NC_P_ROWS(8) NC_P_ROWS(9) NC_P_ROWS(10) NC_P_ROWS(11)
+#undef NC_P_ROWS
+        default: return nullptr;
     }
 }
 
@@ -170,10 +213,10 @@ cudaError_t launch_batch_crt(const BatchCrtArgs& args, bool tensor_cores, size_t
 cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
     cudaError_t e = upload_prime_constants(pc, pow32);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_persistent<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(smax(dec_smem_bytes(kMaxPrimes), row_smem_bytes(kThreads, kBatchRowLogE))));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_persistent<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    for (int n = 1; n <= kBatchRowLogMax && e == cudaSuccess; ++n)
+        e = cudaFuncSetAttribute(persistent_rows_kernel(n), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(row_smem_bytes(kThreads, kBatchRowLogE)));
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_batch_crt, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -186,16 +229,29 @@ cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
 
 // Launch with `ctas` persistent CTAs and `smem` dynamic shared memory; `with_dec` when the queue
 // holds residue items.
-cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s, bool with_dec) {
+cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s) {
     BatchArgs a = args;
     void* params[] = {&a};
-    void* fn = with_dec ? reinterpret_cast<void*>(&k_persistent<true>) : reinterpret_cast<void*>(&k_persistent<false>);
-    return cudaLaunchKernel(fn, dim3(unsigned(ctas)), dim3(kThreads), params, smem, s);
+    return cudaLaunchKernel(reinterpret_cast<void*>(&k_persistent), dim3(unsigned(ctas)), dim3(kThreads), params, smem,
+                            s);
 }
 
-cudaError_t persistent_occupancy(size_t smem, bool with_dec, int* ctas_per_sm) {
-    return with_dec ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_persistent<true>, kThreads, smem)
-                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_persistent<false>, kThreads, smem);
+cudaError_t launch_persistent_rows(const BatchArgs& args, int logN2, int ctas, cudaStream_t s) {
+    BatchArgs a = args;
+    void* params[] = {&a};
+    void* fn = persistent_rows_kernel(logN2);
+    if (!fn) return cudaErrorInvalidValue;
+    return cudaLaunchKernel(fn, dim3(unsigned(ctas)), dim3(kThreads), params, row_smem_bytes(kThreads, kBatchRowLogE), s);
+}
+
+cudaError_t persistent_rows_occupancy(int logN2, int* ctas_per_sm) {
+    void* fn = persistent_rows_kernel(logN2);
+    if (!fn) return cudaErrorInvalidValue;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, kThreads, row_smem_bytes(kThreads, kBatchRowLogE));
+}
+
+cudaError_t persistent_occupancy(size_t smem, int* ctas_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k_persistent, kThreads, smem);
 }
 
 }  // namespace nc

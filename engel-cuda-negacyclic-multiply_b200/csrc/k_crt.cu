@@ -7,6 +7,7 @@ namespace nc {
 template <int LW>
 __global__ void __launch_bounds__(kThreads, 2) k_crt(ProductDesc d, Tables t) {
     extern __shared__ __align__(16) uint8_t smem[];
+    pdl_trigger();
     crt_coeffs<LW>(d, t, int(blockIdx.x), smem);
 }
 

@@ -7,6 +7,7 @@ namespace nc {
 template <int LW>
 __global__ void __launch_bounds__(kThreads, 2) k_crt_tc(ProductDesc d, Tables t) {
 #if NC_HAS_TCGEN05
+    pdl_trigger();
     constexpr uint32_t kCols = crt_tc_tmem_cols(LW);
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;

@@ -10,6 +10,7 @@ namespace nc {
 template <int LW>
 __global__ void __launch_bounds__(kThreads, 3) k_dec(ProductDesc d, Tables t, int first_operand, int tiles) {
     extern __shared__ __align__(16) uint8_t smem[];
+    pdl_trigger();
     const int operand = first_operand + int(blockIdx.x) / tiles;
     const int tile = int(blockIdx.x) % tiles;
     dec_tile<LW>(d, t, operand, tile, smem);

@@ -101,6 +101,10 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
 
+    // B: the weight bytes of the first `groups` primes, already in shared-memory order
+    for (int q = tid; q < groups * 64; q += kThreads) cp_async16(sB + q * 16, t.res_w + q);
+    for (int w = tid; w < k; w += kThreads) s_p[w] = __ldg(t.primes + w);
+    pdl_wait();  // the operand and the residue rows belong to the stream's previous kernels
     // A: 16-byte chunk q = (row group, K chunk, row), row m = u C + j is coefficient u N2 + j0 + j
     const int kbytes = 4 * L;
     for (int q = tid; q < kDecTcRows * 8; q += kThreads) {
@@ -124,9 +128,6 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
             *reinterpret_cast<uint4*>(dst) = make_uint4(0u, 0u, 0u, 0u);
         }
     }
-    // B: the weight bytes of the first `groups` primes, already in shared-memory order
-    for (int q = tid; q < groups * 64; q += kThreads) cp_async16(sB + q * 16, t.res_w + q);
-    for (int w = tid; w < k; w += kThreads) s_p[w] = __ldg(t.primes + w);
     asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy writes -> MMA reads
@@ -269,6 +270,7 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
 template <int LOG_N1>
 __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_dec_tc(ProductDesc d, Tables t, int first_operand, int tiles) {
 #if NC_HAS_TCGEN05
+    pdl_trigger();
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;

@@ -4,9 +4,13 @@
 
 namespace nc {
 
+// Resident CTAs per SM the register allocation aims at: radix-8 passes in 256-thread CTAs fit three
+// (80 registers a thread; k_row<11,3,256> at N = 2^16: 69.6 us against 71.7 us at two), radix-16
+// passes keep two (128 registers; at 80 they spill about 500 bytes a thread).
 template <int LOG_N2, int LOG_E, int THREADS>
-__global__ void __launch_bounds__(THREADS, (THREADS == 256 ? 2 : 1)) k_row(ProductDesc d, Tables t) {
+__global__ void __launch_bounds__(THREADS, (THREADS == 256 ? (LOG_E == 3 ? 3 : 2) : 1)) k_row(ProductDesc d, Tables t) {
     extern __shared__ __align__(16) uint8_t smem[];
+    pdl_trigger();
     row_blocks<LOG_N2, LOG_E, THREADS>(d, t, int(blockIdx.x), smem);
 }
 

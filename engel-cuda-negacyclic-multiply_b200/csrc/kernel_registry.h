@@ -26,11 +26,15 @@ cudaError_t prepare_row(const PrimeConst* pc, const uint64_t* pow32);
 cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32);
 cudaError_t prepare_residues(const PrimeConst* pc, const uint64_t* pow32);
 
-cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s, bool with_dec);
+// Residue and row items (the queue holds residue items of products on the integer residue engine).
+cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s);
 cudaError_t launch_batch_crt(const BatchCrtArgs& args, bool tensor_cores, size_t smem, cudaStream_t s);
 // Residue items of a batch on the tensor cores (BatchCrtArgs items: x = product, y = operand *
 // tiles_tc + tile), every product of the launch with column length 2^logN1.
 cudaError_t launch_batch_dec_tc(const BatchCrtArgs& args, int logN1, size_t smem, cudaStream_t s);
-cudaError_t persistent_occupancy(size_t smem, bool with_dec, int* ctas_per_sm);
+cudaError_t persistent_occupancy(size_t smem, int* ctas_per_sm);
+// Row items alone, all with row blocks of 2^logN2 residues (none waits on another item).
+cudaError_t launch_persistent_rows(const BatchArgs& args, int logN2, int ctas, cudaStream_t s);
+cudaError_t persistent_rows_occupancy(int logN2, int* ctas_per_sm);
 
 }  // namespace nc

@@ -9,9 +9,21 @@ namespace nc {
 
 namespace {
 
+// The product kernels go out with programmatic dependent launch: each may be scheduled while the
+// kernel before it on the stream finishes its last wave (see pdl_wait / pdl_trigger).
 cudaError_t launch(void* fn, int grid, int threads, size_t smem, cudaStream_t s, void** args) {
     if (grid <= 0) return cudaSuccess;
-    return cudaLaunchKernel(fn, dim3(unsigned(grid)), dim3(unsigned(threads)), args, smem, s);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(threads));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 constexpr int kProbeIters = 2048;

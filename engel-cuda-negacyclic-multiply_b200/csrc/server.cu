@@ -91,7 +91,10 @@ Server::Server(int device, size_t hbm_budget, size_t staging_bytes, int max_batc
             batches_.emplace_back(new Batch(device));
             stream_busy_.push_back(false);
         }
+        check(cudaEventCreate(&origin_), "event");
+        check(cudaEventRecord(origin_, streams_[0]), "event");
     } catch (...) {
+        if (origin_) cudaEventDestroy(origin_);
         for (auto s : streams_) cudaStreamDestroy(s);
         batches_.clear();
         cudaFree(dev_base_);
@@ -109,7 +112,11 @@ Server::~Server() {
     cv_.notify_all();
     if (thread_.joinable()) thread_.join();
     for (auto s : streams_) cudaStreamSynchronize(s);
-    for (auto& f : flights_) cudaEventDestroy(f.done);
+    for (auto& f : flights_) {
+        cudaEventDestroy(f.begin);
+        cudaEventDestroy(f.done);
+    }
+    if (origin_) cudaEventDestroy(origin_);
     batches_.clear();
     for (auto s : streams_) cudaStreamDestroy(s);
     cudaFree(dev_base_);
@@ -286,6 +293,34 @@ void Server::stats(double* p50_ms, double* p99_ms, uint64_t* completed, double* 
     if (timeouts) *timeouts = timeouts_;
 }
 
+void Server::io_stats(uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* busy_ms, double* window_ms) {
+    std::lock_guard<std::mutex> lock(mu_);
+    std::vector<std::pair<double, double>> v = busy_;
+    std::sort(v.begin(), v.end());
+    double busy = 0, lo = 0, hi = 0, first = 0, last = 0;
+    bool open = false;
+    for (const auto& iv : v) {
+        if (!open) {
+            lo = iv.first;
+            hi = iv.second;
+            first = iv.first;
+            open = true;
+        } else if (iv.first > hi) {
+            busy += hi - lo;
+            lo = iv.first;
+            hi = iv.second;
+        } else {
+            hi = std::max(hi, iv.second);
+        }
+        last = std::max(last, iv.second);
+    }
+    if (open) busy += hi - lo;
+    if (h2d_bytes) *h2d_bytes = h2d_bytes_;
+    if (d2h_bytes) *d2h_bytes = d2h_bytes_;
+    if (busy_ms) *busy_ms = busy;
+    if (window_ms) *window_ms = open ? last - first : 0.0;
+}
+
 // Scheduler thread: reap finished batches, admit queued requests in order while the HBM budget
 // holds them, launch them as one batch on a free stream. Called with mu_ held.
 void Server::launch(std::vector<Request*>& reqs) {
@@ -318,6 +353,8 @@ void Server::launch(std::vector<Request*>& reqs) {
     if (reqs.empty()) return;
     Flight f;
     try {
+        check(cudaEventCreate(&f.begin), "event");
+        check(cudaEventRecord(f.begin, st), "event");
         for (Request* r : reqs) {
             const size_t bytes = r->plan->limbs() * 4;
             char* da = r->dev;
@@ -326,6 +363,8 @@ void Server::launch(std::vector<Request*>& reqs) {
             uint64_t* scratch = reinterpret_cast<uint64_t*>(r->dev + 3 * r->limb_bytes);
             if (r->operand < 0) check(cudaMemcpyAsync(da, r->host, bytes, cudaMemcpyHostToDevice, st), "operand copy");
             check(cudaMemcpyAsync(db, r->host + r->limb_bytes, bytes, cudaMemcpyHostToDevice, st), "operand copy");
+            f.h2d += bytes * (r->operand < 0 ? 2 : 1);
+            f.d2h += bytes;
             if (r->operand >= 0)
                 batch.add(r->plan, kModeCachedA, nullptr, reinterpret_cast<uint32_t*>(db),
                           reinterpret_cast<uint32_t*>(dc),
@@ -342,12 +381,14 @@ void Server::launch(std::vector<Request*>& reqs) {
                   "product copy");
         f.reqs = reqs;
         f.stream = s;
-        check(cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming), "event");
+        check(cudaEventCreate(&f.done), "event");
         check(cudaEventRecord(f.done, st), "event");
     } catch (...) {
         // copies or kernels of this batch may already be queued: the caller frees the requests'
         // device blocks, so wait until nothing on the stream can still touch them
         cudaStreamSynchronize(st);
+        if (f.begin) cudaEventDestroy(f.begin);
+        if (f.done) cudaEventDestroy(f.done);
         throw;
     }
     stream_busy_[size_t(s)] = true;
@@ -383,7 +424,17 @@ bool Server::reap(bool) {
                 r->status = -1;
             }
         }
-        if (q != cudaSuccess) fault_ = cudaGetErrorString(q);
+        if (q != cudaSuccess) {
+            fault_ = cudaGetErrorString(q);
+        } else {
+            float b = 0.f, e = 0.f;
+            if (cudaEventElapsedTime(&b, origin_, it->begin) == cudaSuccess &&
+                cudaEventElapsedTime(&e, origin_, it->done) == cudaSuccess)
+                busy_.emplace_back(double(b), double(e));
+            h2d_bytes_ += it->h2d;
+            d2h_bytes_ += it->d2h;
+        }
+        cudaEventDestroy(it->begin);
         cudaEventDestroy(it->done);
         stream_busy_[size_t(it->stream)] = false;
         it = flights_.erase(it);

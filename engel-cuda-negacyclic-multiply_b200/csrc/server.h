@@ -54,6 +54,10 @@ class Server {
     double wait(uint64_t id, uint32_t* c);  // milliseconds of latency
     void stats(double* p50_ms, double* p99_ms, uint64_t* completed, double* products_per_s, size_t* hbm_in_use,
                uint64_t* batches, uint64_t* timeouts = nullptr);
+    // Bytes copied host -> device and device -> host for finished batches, and on the device's clock
+    // the time during which at least one batch had copies or kernels in flight (the union of the
+    // batches' intervals) within the window from the first batch's start to the last one's end.
+    void io_stats(uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* busy_ms, double* window_ms);
 
   private:
     struct Request {
@@ -75,8 +79,10 @@ class Server {
     };
     struct Flight {
         std::vector<Request*> reqs;
-        cudaEvent_t done;
+        cudaEvent_t begin = nullptr;  // before the batch's first copy
+        cudaEvent_t done = nullptr;   // after its last copy
         int stream;
+        uint64_t h2d = 0, d2h = 0;
     };
 
     void loop();
@@ -106,6 +112,9 @@ class Server {
     double t_first_ = -1, t_last_ = 0;
     uint64_t batches_run_ = 0;
     uint64_t timeouts_ = 0;  // batches whose dependency wait gave up (their requests fail)
+    cudaEvent_t origin_ = nullptr;                    // device-clock origin of the batch intervals
+    std::vector<std::pair<double, double>> busy_;    // [begin, end) of finished batches, ms from origin_
+    uint64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
     std::string last_timeout_;  // what the last such wait waited for
     std::thread thread_;
 };

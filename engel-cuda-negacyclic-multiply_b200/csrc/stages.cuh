@@ -264,9 +264,10 @@ __device__ void dec_tile(const ProductDesc& d, const Tables& t, int operand, int
     const int j0 = tile * C;
 
     __syncthreads();  // the previous user of shared memory (persistent CTAs) is done
-    load_tile(x, N >> logN1, L, j0, C, 1 << logN1, s_in);
     for (int w = threadIdx.x; w < k * kMaxL; w += blockDim.x) s_pow[w] = __ldg(t.pow32 + w);
     for (int w = threadIdx.x; w < k; w += blockDim.x) s_p[w] = __ldg(t.primes + w);
+    pdl_wait();  // the operand and the residue rows belong to the stream's previous kernels
+    load_tile(x, N >> logN1, L, j0, C, 1 << logN1, s_in);
     __syncthreads();
     dec_residues<LW>(s_in, L, k, T, s_pow, s_res);
     __syncthreads();
@@ -429,6 +430,7 @@ __device__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint
     uint64_t v[S::E];
 
     __syncthreads();  // shared memory of a previous item is free
+    pdl_wait();       // the residues come from the stream's previous kernel
     if (d.mode == kModeCachedA) {
         // a is already in the NTT domain: stage it into buf_a
 #pragma unroll
@@ -643,6 +645,7 @@ __device__ void crt_coeffs(const ProductDesc& d, const Tables& t, int tile, uint
     }
     if (threadIdx.x < 4) s_mu[threadIdx.x] = __ldg(qc->mu + threadIdx.x);
     __syncthreads();  // s_p is read by the column stages
+    pdl_wait();       // the residues come from the stream's previous kernel
 
     switch (logN1) {
         case 0: crt_columns<0>(d, t, tile, s_p, s_res); break;
