@@ -405,8 +405,10 @@ void ensure_host_path(Plan* p) {
     }
     // one set of copy threads per process, shared by every plan (jobs run one at a time)
     static HostPool* shared = new HostPool(copy_threads());
-    p->ev_out.assign(size_t(shared->parts()), nullptr);
+    p->ev_out.assign(size_t(kMaxOutChunks), nullptr);
     for (auto& ev : p->ev_out) check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+    p->ev_grp.assign(4, nullptr);
+    for (auto& ev : p->ev_grp) check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
     check(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
     check(cudaEventCreateWithFlags(&p->ev_a, cudaEventDisableTiming), "event");
     check(cudaEventCreateWithFlags(&p->ev_b, cudaEventDisableTiming), "event");
@@ -443,6 +445,8 @@ void plan_destroy(Plan* p) {
     if (p->stream) cudaStreamDestroy(p->stream);
     for (auto ev : p->ev_out)
         if (ev) cudaEventDestroy(ev);
+    for (auto ev : p->ev_grp)
+        if (ev) cudaEventDestroy(ev);
     release_tables(p->tables);
     delete p;
 }
@@ -470,16 +474,62 @@ void slice(size_t bytes, int part, int parts, size_t* lo, size_t* hi) {
 }
 
 // Host-to-device copies of a few MB each: on PCIe 5 hosts, copies of a few hundred KB reach well
-// under half the link rate (per-copy overhead), and multi-MB copies reach most of it.
+// under half the link rate (per-copy overhead), and multi-MB copies reach most of it. The first
+// operand's chunks grow from 512 KB (512 KB, 1, 2, 4, 4 ... MB): the link idles only while the
+// first, small chunk is staged (staging runs at about 1.8 times the link rate, so each chunk is
+// staged while the one before it transfers), where one 4 MB first chunk left it idle ~40 us.
 constexpr size_t kDmaChunk = size_t(4) << 20;
+constexpr size_t kFirstChunk = size_t(512) << 10;
 
-// The product comes back in at most `parts` device-to-host copies of about 2 MB or more (one
-// event each); returns their number and writes their size (a multiple of 4 KiB).
-int out_chunks(size_t bytes, int parts, size_t* chunk) {
-    const size_t want = bytes / (size_t(2) << 20);
-    const int n = int(std::max<size_t>(1, std::min<size_t>(want, size_t(parts))));
-    *chunk = ((bytes + size_t(n) - 1) / size_t(n) + 4095) / 4096 * 4096;
-    return int((bytes + *chunk - 1) / *chunk);
+std::vector<std::pair<size_t, size_t>> upload_chunks(size_t bytes, bool ramp) {
+    std::vector<std::pair<size_t, size_t>> out;
+    size_t want = ramp ? kFirstChunk : kDmaChunk;
+    for (size_t off = 0; off < bytes;) {
+        size_t len = std::min(want, bytes - off);
+        if (bytes - off - len < want / 2) len = bytes - off;  // no small last chunk
+        out.emplace_back(off, len);
+        off += len;
+        want = std::min(kDmaChunk, 2 * want);
+    }
+    return out;
+}
+
+// The product comes back in device-to-host copies that shrink towards the end (the rest, then
+// 2.5 MB pieces, 1 MB, 384 KB; one event each): every chunk's copy-out into the caller's buffer
+// overlaps the next chunk's transfer, so what follows the last transfer is the copy-out of a
+// 384 KB chunk (three equal 2.5 MB chunks left ~40 us of copy-out after the last one landed;
+// chunks of 1 MB and less transfer at only 30-40 GB/s, so the others stay large).
+std::vector<std::pair<size_t, size_t>> download_chunks(size_t bytes) {
+    std::vector<size_t> lens;  // from the last chunk backwards
+    const size_t tail[] = {size_t(384) << 10, size_t(1) << 20};
+    size_t left = bytes;
+    for (size_t t : tail) {
+        if (left <= t + (t >> 1)) break;
+        lens.push_back(t);
+        left -= t;
+    }
+    const size_t piece = size_t(5) << 19;
+    while (left > piece + (piece >> 1) && int(lens.size()) < kMaxOutChunks - 1) {
+        lens.push_back(piece);
+        left -= piece;
+    }
+    if (left) lens.push_back(left);
+    std::vector<std::pair<size_t, size_t>> out;
+    size_t off = 0;
+    for (auto it = lens.rbegin(); it != lens.rend(); ++it) {
+        out.emplace_back(off, *it);
+        off += *it;
+    }
+    return out;
+}
+
+// Operand b of a pair goes up in this many column groups, each a strided copy of its columns of
+// every row segment, and each group's residue tiles start as soon as it has landed: the residue
+// stage of b then ends about one group's tiles after the last byte, not a whole stage after.
+int upload_groups(const Plan* p, const ProductDesc& d) {
+    constexpr int kGroups = 4;
+    if (p->N < (1 << 13)) return 1;
+    return residue_tiles(d, p->cfg) % kGroups == 0 ? kGroups : 1;
 }
 
 }  // namespace
@@ -493,12 +543,10 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
         if (!x[f]) throw Error(kEInval, "null host buffer");
     ensure_host_path(p);
     const size_t bytes = p->limbs() * sizeof(uint32_t);
-    // Each operand goes in equal chunks of at most kDmaChunk: every copy thread stages its part of
-    // a chunk into pinned memory, then the chunk's DMA is enqueued and runs while the next chunk
-    // is staged. Operand a goes on the plan's stream; operand b on the copy stream, after a's
-    // upload (so a arrives first at full link rate), and a's residue stage runs while b uploads.
-    const size_t nchunks = (bytes + kDmaChunk - 1) / kDmaChunk;
-    const size_t chunk = ((bytes + nchunks - 1) / nchunks + 4095) / 4096 * 4096;
+    // Each operand goes in chunks: every copy thread stages its part of a chunk into pinned memory,
+    // then the chunk's DMA is enqueued and runs while the next chunk is staged. Operand a goes on
+    // the plan's stream; operand b on the copy stream, after a's upload (so a arrives first at full
+    // link rate), and a's stages run while b uploads.
     const char* srcs[kMaxFactors];
     char* pins[kMaxFactors];
     char* devs[kMaxFactors];
@@ -511,6 +559,7 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
         devs[f] = reinterpret_cast<char*>(dev_ops[f]);
     }
     ProductDesc d = n == 2 ? p->desc(p->d_a, p->d_b, p->d_c) : p->desc_chain(dev_ops, p->d_c);
+    int groups = 1;  // column groups of b's upload (pairs only)
     for (int op = 0; op < n; ++op) {
         cudaStream_t stream = op == 0 ? p->stream : p->copy_stream;
         if (op == 1) {
@@ -534,34 +583,59 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
                 d.mode = kModeCachedA;
                 d.a = nullptr;
                 d.a_hat = p->d_hat;
+                groups = upload_groups(p, d);
             } else {
                 check(launch_residues(d, p->tables->view(), p->cfg, p->stream, 0, 1), "kernel launch");
             }
             check(cudaStreamWaitEvent(p->copy_stream, p->ev_a, 0), "stream wait");
         }
-        for (size_t off = 0; off < bytes; off += chunk) {
-            const size_t len = std::min(chunk, bytes - off);
+        const bool grouped = op == 1 && groups > 1;
+        for (const auto& ch : upload_chunks(bytes, op == 0)) {
+            const size_t off = ch.first, len = ch.second;
             p->pool->run([&](int part, int parts) {
                 size_t lo, hi;
                 slice(len, part, parts, &lo, &hi);
                 if (hi > lo) stage_copy(pins[op] + off + lo, srcs[op] + off + lo, hi - lo);
             });
-            check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, len, cudaMemcpyHostToDevice, stream),
-                  "operand copy");
+            if (!grouped)
+                check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, len, cudaMemcpyHostToDevice, stream),
+                      "operand copy");
+        }
+        if (grouped) {
+            // b is staged whole (while a transfers); group g is columns [g N2 / G, (g + 1) N2 / G) of
+            // every row segment, one strided copy, then its residue tiles on the plan's stream
+            const int logN1 = p->logN - p->cfg.logN2;
+            const size_t N2 = size_t(1) << p->cfg.logN2, row = N2 * size_t(p->L) * 4;
+            const size_t width = row / size_t(groups);
+            for (int g = 0; g < groups; ++g) {
+                check(cudaMemcpy2DAsync(devs[op] + size_t(g) * width, row, pins[op] + size_t(g) * width, row, width,
+                                        size_t(1) << logN1, cudaMemcpyHostToDevice, stream),
+                      "operand copy");
+                check(cudaEventRecord(p->ev_grp[size_t(g)], stream), "event");
+            }
         }
     }
     check(cudaEventRecord(p->ev_b, p->copy_stream), "event");
-    check(launch_product(d, p->tables->view(), p->cfg, p->stream, p->timing ? p->ev_stage : nullptr, p->ev_b),
-          "kernel launch");
+    if (groups > 1) {
+        if (p->timing) check(cudaEventRecord(p->ev_stage[0], p->stream), "event");
+        for (int g = 0; g < groups; ++g) {
+            check(cudaStreamWaitEvent(p->stream, p->ev_grp[size_t(g)], 0), "stream wait");
+            check(launch_residues(d, p->tables->view(), p->cfg, p->stream, 1, 1, g, groups), "kernel launch");
+        }
+        cudaEvent_t* ev = p->timing ? p->ev_stage : nullptr;
+        check(launch_product(d, p->tables->view(), p->cfg, p->stream, ev, nullptr, true), "kernel launch");
+    } else {
+        check(launch_product(d, p->tables->view(), p->cfg, p->stream, p->timing ? p->ev_stage : nullptr, p->ev_b),
+              "kernel launch");
+    }
     check(cudaEventRecord(p->ev_stop, p->stream), "event");
-    size_t out_chunk;
-    const int nd = out_chunks(bytes, p->pool->parts(), &out_chunk);
-    for (int j = 0; j < nd; ++j) {
-        const size_t lo = size_t(j) * out_chunk, n = std::min(out_chunk, bytes - lo);
-        check(cudaMemcpyAsync(reinterpret_cast<char*>(p->h_c) + lo, reinterpret_cast<char*>(p->d_c) + lo, n,
-                              cudaMemcpyDeviceToHost, p->stream),
+    const auto out = download_chunks(bytes);
+    for (size_t j = 0; j < out.size(); ++j) {
+        check(cudaMemcpyAsync(reinterpret_cast<char*>(p->h_c) + out[j].first,
+                              reinterpret_cast<char*>(p->d_c) + out[j].first, out[j].second, cudaMemcpyDeviceToHost,
+                              p->stream),
               "product copy");
-        check(cudaEventRecord(p->ev_out[size_t(j)], p->stream), "event");
+        check(cudaEventRecord(p->ev_out[j], p->stream), "event");
     }
 }
 
@@ -577,9 +651,8 @@ void plan_collect_host(Plan* p, uint32_t* c) {
     if (!c) throw Error(kEInval, "null host buffer");
     if (!p->pool) throw Error(kEInval, "collect without a submitted product");
     const size_t bytes = p->limbs() * sizeof(uint32_t);
-    size_t out_chunk;
-    out_chunks(bytes, p->pool->parts(), &out_chunk);
-    const int nd = int((bytes + out_chunk - 1) / out_chunk);
+    const auto out = download_chunks(bytes);
+    const int nd = int(out.size());
     std::atomic<int> err{int(cudaSuccess)};
     // Every copy thread takes its share of each chunk as soon as that chunk has landed, so the
     // copy-out after the last transfer is one chunk split over all threads. Only the calling
@@ -605,7 +678,7 @@ void plan_collect_host(Plan* p, uint32_t* c) {
                 }
                 if (seen > nd) return;
             }
-            const size_t base = size_t(j) * out_chunk, n = std::min(out_chunk, bytes - base);
+            const size_t base = out[size_t(j)].first, n = out[size_t(j)].second;
             size_t lo, hi;
             slice(n, part, parts, &lo, &hi);
             if (hi > lo)

@@ -75,6 +75,9 @@ class HostPool {
     const std::function<void(int, int)>* job_ = nullptr;
 };
 
+// Device-to-host copies (and events) of one product on the host path, at most.
+constexpr int kMaxOutChunks = 16;
+
 // One (N, q) configuration: constants, scratch residues and staging buffers.
 struct Plan {
     int device = 0;
@@ -96,7 +99,8 @@ struct Plan {
     uint64_t* d_hat = nullptr;  // host path: NTT form of operand a (k x N), made while b uploads
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
-    std::vector<cudaEvent_t> ev_out;  // one per output chunk (one chunk per pool part)
+    std::vector<cudaEvent_t> ev_out;  // one per output chunk
+    std::vector<cudaEvent_t> ev_grp;  // host path: a column group of operand b has landed
     cudaStream_t copy_stream = nullptr;         // host path: operand b's upload
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // operand a uploaded / operand b uploaded
     DeviceTables* tables = nullptr;

@@ -85,6 +85,7 @@ __device__ __forceinline__ void batch_item(uint32_t stage, const BatchProduct& b
 // item, and the stages read its fields from there.
 __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
+    pdl_trigger();
     __shared__ int s_item;
     __shared__ int s_go;
     __shared__ __align__(16) BatchProduct s_bp;
@@ -124,6 +125,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_persistent(BatchArgs a) {
 template <int LOG_N2>
 __global__ void __launch_bounds__(kThreads, 3) k_persistent_rows(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
+    pdl_trigger();
     __shared__ int s_item;
     __shared__ __align__(16) BatchProduct s_bp;
     constexpr int kWords = int(sizeof(BatchProduct) / 4);
@@ -155,6 +157,7 @@ static void* persistent_rows_kernel(int logN2) {
 
 __global__ void __launch_bounds__(kThreads, 2) k_batch_crt(BatchCrtArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
+    pdl_trigger();
     const uint2 w = __ldg(a.items + blockIdx.x);
     const BatchProduct& bp = a.products[w.x];
     switch (bp.d.LW) {
@@ -168,6 +171,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_crt(BatchCrtArgs a) {
 
 __global__ void __launch_bounds__(kThreads, 2) k_batch_crt_tc(BatchCrtArgs a) {
 #if NC_HAS_TCGEN05
+    pdl_trigger();
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
@@ -207,7 +211,7 @@ cudaError_t launch_batch_crt(const BatchCrtArgs& args, bool tensor_cores, size_t
     BatchCrtArgs a = args;
     void* params[] = {&a};
     void* fn = tensor_cores ? reinterpret_cast<void*>(&k_batch_crt_tc) : reinterpret_cast<void*>(&k_batch_crt);
-    return cudaLaunchKernel(fn, dim3(unsigned(args.n_items)), dim3(kThreads), params, smem, s);
+    return launch_pdl(fn, args.n_items, kThreads, smem, s, params);
 }
 
 cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
@@ -232,8 +236,7 @@ cudaError_t prepare_persistent(const PrimeConst* pc, const uint64_t* pow32) {
 cudaError_t launch_persistent(const BatchArgs& args, int ctas, size_t smem, cudaStream_t s) {
     BatchArgs a = args;
     void* params[] = {&a};
-    return cudaLaunchKernel(reinterpret_cast<void*>(&k_persistent), dim3(unsigned(ctas)), dim3(kThreads), params, smem,
-                            s);
+    return launch_pdl(reinterpret_cast<void*>(&k_persistent), ctas, kThreads, smem, s, params);
 }
 
 cudaError_t launch_persistent_rows(const BatchArgs& args, int logN2, int ctas, cudaStream_t s) {
@@ -241,7 +244,7 @@ cudaError_t launch_persistent_rows(const BatchArgs& args, int logN2, int ctas, c
     void* params[] = {&a};
     void* fn = persistent_rows_kernel(logN2);
     if (!fn) return cudaErrorInvalidValue;
-    return cudaLaunchKernel(fn, dim3(unsigned(ctas)), dim3(kThreads), params, row_smem_bytes(kThreads, kBatchRowLogE), s);
+    return launch_pdl(fn, ctas, kThreads, row_smem_bytes(kThreads, kBatchRowLogE), s, params);
 }
 
 cudaError_t persistent_rows_occupancy(int logN2, int* ctas_per_sm) {

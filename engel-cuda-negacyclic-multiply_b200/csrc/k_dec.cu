@@ -8,11 +8,11 @@ namespace nc {
 // the residue loop is latency bound, and the third CTA's warps hide more of it than the
 // registers it costs (measured at N = 65536, 868-bit q: 78.1 -> 75.1 us).
 template <int LW>
-__global__ void __launch_bounds__(kThreads, 3) k_dec(ProductDesc d, Tables t, int first_operand, int tiles) {
+__global__ void __launch_bounds__(kThreads, 3) k_dec(ProductDesc d, Tables t, int first_operand, int tile0, int tiles) {
     extern __shared__ __align__(16) uint8_t smem[];
     pdl_trigger();
     const int operand = first_operand + int(blockIdx.x) / tiles;
-    const int tile = int(blockIdx.x) % tiles;
+    const int tile = tile0 + int(blockIdx.x) % tiles;
     dec_tile<LW>(d, t, operand, tile, smem);
 }
 

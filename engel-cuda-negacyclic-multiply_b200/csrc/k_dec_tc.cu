@@ -266,15 +266,16 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
 // columns, and 32-point columns on two lanes) take three.
 #define NC_DEC_TC_BOUNDS(LOG_N1) __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : 3)
 
-// Plain path: one product, grid = operands x tiles.
+// Plain path: one product, grid = operands x tiles, tiles tile0 .. tile0 + tiles - 1 of each operand.
 template <int LOG_N1>
-__global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_dec_tc(ProductDesc d, Tables t, int first_operand, int tiles) {
+__global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_dec_tc(ProductDesc d, Tables t, int first_operand, int tile0, int tiles) {
 #if NC_HAS_TCGEN05
     pdl_trigger();
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
-    dec_tc_item<LOG_N1>(d, t, first_operand + int(blockIdx.x) / tiles, int(blockIdx.x) % tiles, smem, bar, taddr_slot);
+    dec_tc_item<LOG_N1>(d, t, first_operand + int(blockIdx.x) / tiles, tile0 + int(blockIdx.x) % tiles, smem, bar,
+                        taddr_slot);
 #endif
 }
 
@@ -283,6 +284,7 @@ __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_dec_tc(ProductDesc d, Tables t, int f
 template <int LOG_N1>
 __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_batch_dec_tc(BatchCrtArgs a) {
 #if NC_HAS_TCGEN05
+    pdl_trigger();
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
@@ -338,7 +340,7 @@ cudaError_t launch_batch_dec_tc(const BatchCrtArgs& args, int logN1, size_t smem
     if (args.n_items <= 0) return cudaSuccess;
     BatchCrtArgs a = args;
     void* params[] = {&a};
-    return cudaLaunchKernel(fn, dim3(unsigned(args.n_items)), dim3(kThreads), params, smem, s);
+    return launch_pdl(fn, args.n_items, kThreads, smem, s, params);
 }
 
 }  // namespace nc

@@ -11,6 +11,24 @@
 
 namespace nc {
 
+// Launch with programmatic dependent launch allowed: the kernel may be scheduled once every CTA
+// of the kernel before it on the stream has called pdl_trigger(), and waits for that kernel's
+// results in pdl_wait() (both in arith.cuh).
+inline cudaError_t launch_pdl(const void* fn, int grid, int threads, size_t smem, cudaStream_t s, void** args) {
+    if (grid <= 0) return cudaSuccess;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(threads));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 void* dec_kernel(int LW);
 void* dec_tc_kernel(int logN1);
 void* crt_kernel(int LW);

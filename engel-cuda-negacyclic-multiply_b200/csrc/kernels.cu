@@ -12,18 +12,7 @@ namespace {
 // The product kernels go out with programmatic dependent launch: each may be scheduled while the
 // kernel before it on the stream finishes its last wave (see pdl_wait / pdl_trigger).
 cudaError_t launch(void* fn, int grid, int threads, size_t smem, cudaStream_t s, void** args) {
-    if (grid <= 0) return cudaSuccess;
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(unsigned(grid));
-    cfg.blockDim = dim3(unsigned(threads));
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, fn, args);
+    return launch_pdl(fn, grid, threads, smem, s, args);
 }
 
 constexpr int kProbeIters = 2048;
@@ -67,29 +56,37 @@ cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32) {
     return e;
 }
 
+int residue_tiles(const ProductDesc& d, const RowConfig& cfg) {
+    if (d.res_tc) {
+        const int n = 1 << d.logN;
+        return n < kDecTcRows ? 1 : n / kDecTcRows;
+    }
+    return geometry(int(d.logN), int(d.k), cfg).tiles;
+}
+
 cudaError_t launch_residues(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s, int first,
-                            int count) {
+                            int count, int group, int groups) {
     ProductDesc dd = d;
     Tables tt = t;
-    if (d.res_tc && t.res_w) {
+    if (d.res_tc && !t.res_w) return cudaErrorInvalidValue;
+    const int all = residue_tiles(d, cfg);
+    if (groups < 1 || group < 0 || group >= groups || all % groups != 0) return cudaErrorInvalidValue;
+    int tiles = all / groups;
+    int tile0 = group * tiles;
+    void* args[] = {&dd, &tt, &first, &tile0, &tiles};
+    if (d.res_tc) {
         // tensor-core residues: 128-coefficient tiles
         void* dec = dec_tc_kernel(int(d.logN) - cfg.logN2);
         if (!dec) return cudaErrorInvalidValue;
-        const int n = 1 << d.logN;
-        int tiles = n < kDecTcRows ? 1 : n / kDecTcRows;
-        void* args[] = {&dd, &tt, &first, &tiles};
         return launch(dec, count * tiles, kThreads, dec_tc_smem_bytes(int(d.k)), s, args);
     }
     void* dec = dec_kernel(int(d.LW));
     if (!dec) return cudaErrorInvalidValue;
-    const Geometry g = geometry(int(d.logN), int(d.k), cfg);
-    int tiles = g.tiles;
-    void* args[] = {&dd, &tt, &first, &tiles};
-    return launch(dec, count * g.tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);
+    return launch(dec, count * tiles, kThreads, dec_smem_bytes(int(d.k)), s, args);
 }
 
 cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s,
-                           cudaEvent_t* ev, cudaEvent_t b_ready) {
+                           cudaEvent_t* ev, cudaEvent_t b_ready, bool residues_done) {
     if (int(d.logN2) != cfg.logN2) return cudaErrorInvalidValue;
     void* row = row_kernel(cfg);
     void* crt = d.crt_b ? crt_tc_kernel(int(d.LW)) : crt_kernel(int(d.LW));
@@ -99,7 +96,9 @@ cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfi
     Tables tt = t;
     cudaError_t e;
     const int factors = d.mode == kModeProduct ? int(d.factors) : 1;
-    if (b_ready && d.mode != kModeForward) {
+    if (residues_done) {
+        // every operand's residue stage is already on s (the host path's grouped upload)
+    } else if (b_ready && d.mode != kModeForward) {
         // operand a is already taken care of on s (its residues, or its NTT form for a cached-a
         // product); the other operands follow once they have landed
         if ((e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
