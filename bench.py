@@ -748,7 +748,7 @@ def uneven_batch(dev, mix, args) -> dict:
             "speedup": ms_plain / ms_batch, "bit_exact_vs_plain": exact}
 
 
-def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
+def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600, streams=3, max_batch=64) -> dict:
     """Poisson arrivals of the uneven mix at each rate; 30% of requests reuse one of 8 registered
     operands (NTT form cached on the device); admission by a 40 GB HBM budget. The same arrival
     schedule is also served by the plain per-call form (one worker, fherma_run-style host calls)."""
@@ -768,7 +768,8 @@ def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
         plans.append((nc.Plan(N, cases.limbs_of(q, L)), q, L))
     host = [(cases.coeffs(q, p.N, L, 13000 + i), cases.coeffs(q, p.N, L, 14000 + i)) for i, (p, q, L) in
             enumerate(plans)]
-    out = {"budget_bytes": 40 << 30, "requests_per_rate": requests, "reuse_fraction": 0.3, "rates": []}
+    out = {"budget_bytes": 40 << 30, "requests_per_rate": requests, "reuse_fraction": 0.3, "streams": streams,
+           "max_batch": max_batch, "rates": []}
     try:
         # every request of plan i multiplies host[i]: one expected product per plan (this also
         # allocates each plan's staging before any timing)
@@ -781,7 +782,7 @@ def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
                 pi = rng.randrange(len(plans))
                 sched.append((t, pi, rng.random() < 0.3 and pi < 8))
             row = {"rate_per_s": rate}
-            with nc.Server(hbm_budget=40 << 30, staging=2 << 30, max_batch=64, streams=3) as srv:
+            with nc.Server(hbm_budget=40 << 30, staging=2 << 30, max_batch=max_batch, streams=streams) as srv:
                 opids = {i: srv.register_operand(plans[i][0], host[i][0]) for i in range(8)}
                 clients = 8  # independent Poisson clients (their superposition is Poisson at `rate`)
                 t0 = time.perf_counter()
@@ -829,7 +830,9 @@ def serving(dev, mix, args, rates=(2000, 8000, 16000), requests=600) -> dict:
                              "d2h_gbs": io["d2h_bytes"] / win / 1e9 if win else None,
                              "device_busy_frac": io["device_busy_ms"] / io["device_window_ms"]
                              if io["device_window_ms"] else None,
-                             "batch_size_mean": len(lat_srv) / st["batches"] if st["batches"] else None}
+                             "batch_size_mean": len(lat_srv) / st["batches"] if st["batches"] else None,
+                             "scheduler_busy_frac": io["scheduler_ms"] / io["device_window_ms"]
+                             if io["device_window_ms"] else None}
             # plain per-call form on the same schedule: one worker, host operands in and out
             lat = []
             t0 = time.perf_counter()

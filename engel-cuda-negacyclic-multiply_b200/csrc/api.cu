@@ -519,10 +519,10 @@ int nc_server_stats(nc_server* server, double* p50_ms, double* p99_ms, uint64_t*
 }
 
 int nc_server_io_stats(nc_server* server, uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* device_busy_ms,
-                       double* device_window_ms) {
+                       double* device_window_ms, double* scheduler_ms) {
     return guarded([&] {
         if (!server) throw nc::Error(nc::kEInval, "null server");
-        server->s->io_stats(h2d_bytes, d2h_bytes, device_busy_ms, device_window_ms);
+        server->s->io_stats(h2d_bytes, d2h_bytes, device_busy_ms, device_window_ms, scheduler_ms);
     });
 }
 

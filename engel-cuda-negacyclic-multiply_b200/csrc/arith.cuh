@@ -19,11 +19,11 @@ __device__ __forceinline__ uint64_t csub(uint64_t x, uint64_t m) { return x >= m
 
 // Programmatic dependent launch. A product kernel launched with it may be scheduled while the
 // kernel before it on the stream still runs (once every CTA of that kernel has called
-// pdl_trigger(), which each product kernel does on entry), so its prologue (tensor-memory
-// allocation, constant tables) overlaps that kernel's last wave. pdl_wait() returns once the
-// kernel before has completed and its writes are visible; every read or write of data that
-// kernel produces or consumes comes after it. In a kernel launched without the attribute, both
-// return at once.
+// pdl_trigger(): on entry, or, in kernels that allocate tensor memory, once the CTA holds it), so
+// its prologue (tensor-memory allocation, constant tables) overlaps that kernel's last wave.
+// pdl_wait() returns once the kernel before has completed and its writes are visible; every read
+// or write of data that kernel produces or consumes comes after it. In a kernel launched without
+// the attribute, both return at once.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 

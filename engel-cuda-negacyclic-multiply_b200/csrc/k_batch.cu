@@ -171,7 +171,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_crt(BatchCrtArgs a) {
 
 __global__ void __launch_bounds__(kThreads, 2) k_batch_crt_tc(BatchCrtArgs a) {
 #if NC_HAS_TCGEN05
-    pdl_trigger();
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
@@ -188,6 +187,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_crt_tc(BatchCrtArgs a) {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // triggered only once the CTA holds its tensor memory (see k_dec_tc.cu)
+    pdl_trigger();
     const uint32_t taddr = taddr_slot;
     const uint2 w = __ldg(a.items + blockIdx.x);
     const BatchProduct& bp = a.products[w.x];

@@ -7,7 +7,6 @@ namespace nc {
 template <int LW>
 __global__ void __launch_bounds__(kThreads, 2) k_crt_tc(ProductDesc d, Tables t) {
 #if NC_HAS_TCGEN05
-    pdl_trigger();
     constexpr uint32_t kCols = crt_tc_tmem_cols(LW);
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
@@ -26,6 +25,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_crt_tc(ProductDesc d, Tables t)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // triggered only once the CTA holds its tensor memory (see k_dec_tc.cu)
+    pdl_trigger();
     const uint32_t taddr = taddr_slot;
     crt_coeffs_tc<LW>(d, t, int(blockIdx.x), smem, taddr, &bar, 0);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -100,6 +100,11 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // The next kernel on the stream may be scheduled only once every CTA of this one holds its
+    // tensor memory: a dependent that allocates before its griddepcontrol.wait could otherwise
+    // take the columns a CTA of this kernel still waits for, and each would wait on the other.
+    __syncthreads();
+    pdl_trigger();
 
     // B: the weight bytes of the first `groups` primes, already in shared-memory order
     for (int q = tid; q < groups * 64; q += kThreads) cp_async16(sB + q * 16, t.res_w + q);
@@ -270,7 +275,6 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
 template <int LOG_N1>
 __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_dec_tc(ProductDesc d, Tables t, int first_operand, int tile0, int tiles) {
 #if NC_HAS_TCGEN05
-    pdl_trigger();
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
@@ -284,7 +288,6 @@ __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_dec_tc(ProductDesc d, Tables t, int f
 template <int LOG_N1>
 __global__ void NC_DEC_TC_BOUNDS(LOG_N1) k_batch_dec_tc(BatchCrtArgs a) {
 #if NC_HAS_TCGEN05
-    pdl_trigger();
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;

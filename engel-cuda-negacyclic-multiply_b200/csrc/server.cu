@@ -293,7 +293,8 @@ void Server::stats(double* p50_ms, double* p99_ms, uint64_t* completed, double* 
     if (timeouts) *timeouts = timeouts_;
 }
 
-void Server::io_stats(uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* busy_ms, double* window_ms) {
+void Server::io_stats(uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* busy_ms, double* window_ms,
+                      double* scheduler_ms) {
     std::lock_guard<std::mutex> lock(mu_);
     std::vector<std::pair<double, double>> v = busy_;
     std::sort(v.begin(), v.end());
@@ -319,6 +320,7 @@ void Server::io_stats(uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* busy_ms,
     if (d2h_bytes) *d2h_bytes = d2h_bytes_;
     if (busy_ms) *busy_ms = busy;
     if (window_ms) *window_ms = open ? last - first : 0.0;
+    if (scheduler_ms) *scheduler_ms = launch_ms_;
 }
 
 // Scheduler thread: reap finished batches, admit queued requests in order while the HBM budget
@@ -462,8 +464,10 @@ void Server::loop() {
             }
         }
         if (!admit.empty()) {
+            const double t_launch = now_ms();
             try {
                 launch(admit);
+                launch_ms_ += now_ms() - t_launch;
             } catch (const Error& e) {
                 fault_ = e.what();
                 for (Request* r : admit) {

@@ -57,7 +57,8 @@ class Server {
     // Bytes copied host -> device and device -> host for finished batches, and on the device's clock
     // the time during which at least one batch had copies or kernels in flight (the union of the
     // batches' intervals) within the window from the first batch's start to the last one's end.
-    void io_stats(uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* busy_ms, double* window_ms);
+    void io_stats(uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* busy_ms, double* window_ms,
+                  double* scheduler_ms = nullptr);
 
   private:
     struct Request {
@@ -115,6 +116,7 @@ class Server {
     cudaEvent_t origin_ = nullptr;                    // device-clock origin of the batch intervals
     std::vector<std::pair<double, double>> busy_;    // [begin, end) of finished batches, ms from origin_
     uint64_t h2d_bytes_ = 0, d2h_bytes_ = 0;
+    double launch_ms_ = 0;  // host time the scheduler thread spent enqueueing batches
     std::string last_timeout_;  // what the last such wait waited for
     std::thread thread_;
 };

@@ -79,7 +79,7 @@ C_SYMBOLS = [
     ("nc_server_stats", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _u64p,
                                        ctypes.POINTER(ctypes.c_double), _u64p, _u64p, _u64p]),
     ("nc_server_io_stats", ctypes.c_int, [_vp, _u64p, _u64p, ctypes.POINTER(ctypes.c_double),
-                                          ctypes.POINTER(ctypes.c_double)]),
+                                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
 ]
 
 _lib: ctypes.CDLL | None = None
@@ -403,14 +403,15 @@ class Server:
                 "hbm_in_use": hbm.value, "batches": batches.value, "timeouts": tmo.value}
 
     def io_stats(self) -> dict:
-        """Bytes each way of finished batches, and the device-clock time any batch had copies or
-        kernels in flight within the window from the first batch's start to the last one's end."""
+        """Bytes each way of finished batches, the device-clock time any batch had copies or kernels
+        in flight within the window from the first batch's start to the last one's end, and the host
+        time the scheduler thread spent enqueueing batches."""
         up, down = ctypes.c_uint64(), ctypes.c_uint64()
-        busy, window = ctypes.c_double(), ctypes.c_double()
+        busy, window, sched = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _check(load().nc_server_io_stats(self._h, ctypes.byref(up), ctypes.byref(down), ctypes.byref(busy),
-                                         ctypes.byref(window)))
+                                         ctypes.byref(window), ctypes.byref(sched)))
         return {"h2d_bytes": up.value, "d2h_bytes": down.value, "device_busy_ms": busy.value,
-                "device_window_ms": window.value}
+                "device_window_ms": window.value, "scheduler_ms": sched.value}
 
     def close(self) -> None:
         if self._h:

@@ -244,13 +244,14 @@ int nc_server_wait(nc_server* server, uint64_t request_id, uint32_t* c, double* 
    dependency wait gave up (their requests fail with NC_ETIMEOUT). Pointers may be NULL. */
 int nc_server_stats(nc_server* server, double* p50_ms, double* p99_ms, uint64_t* completed, double* products_per_s,
                     uint64_t* hbm_in_use, uint64_t* batches, uint64_t* timeouts);
-/* Where the served time goes: bytes copied host -> device and device -> host by finished batches,
-   and, on the device's clock, the time during which at least one batch had copies or kernels in
-   flight (the union of the batches' intervals from first copy to last copy) within the window from
-   the first batch's start to the last batch's end. Pointers may be NULL. No counterpart in the
-   reference, which serves nothing. */
+/* Where the served time goes: bytes copied host -> device and device -> host by finished batches;
+   on the device's clock, the time during which at least one batch had copies or kernels in flight
+   (the union of the batches' intervals from first copy to last copy) within the window from the
+   first batch's start to the last batch's end; and the host time the scheduler thread spent
+   enqueueing batches. Pointers may be NULL. No counterpart in the reference, which serves
+   nothing. */
 int nc_server_io_stats(nc_server* server, uint64_t* h2d_bytes, uint64_t* d2h_bytes, double* device_busy_ms,
-                       double* device_window_ms);
+                       double* device_window_ms, double* scheduler_ms);
 
 #ifdef __cplusplus
 }
