@@ -267,9 +267,10 @@ __device__ __forceinline__ void dec_tc_item(const ProductDesc& d, const Tables& 
     }
 }
 
-// Four CTAs per SM where the column transform fits 64 registers; 16 values per thread (16-point
-// columns, and 32-point columns on two lanes) take three.
-#define NC_DEC_TC_BOUNDS(LOG_N1) __launch_bounds__(kThreads, LOG_N1 < 4 ? 4 : 3)
+// Four CTAs per SM (64 registers; tensor memory holds four). The 32-point columns (two lanes of
+// 16 values each) spill about 130 bytes a thread there, and still run faster than at three CTAs
+// (80 registers, no spills): N = 2^16, both operands, 47.1 -> 45.1 us.
+#define NC_DEC_TC_BOUNDS(LOG_N1) __launch_bounds__(kThreads, 4)
 
 // Plain path: one product, grid = operands x tiles, tiles tile0 .. tile0 + tiles - 1 of each operand.
 template <int LOG_N1>
