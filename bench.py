@@ -206,14 +206,18 @@ def make_case_dir(root: Path, case, count: int) -> None:
     (root / "manifest.json").write_text(json.dumps({"N": case.N, "W": case.W, "L": case.L, "cases": count}))
 
 
-def run_harness(binary: Path, case, warmup: int, steps: int, timeout: float = 600.0):
+def run_harness(binary: Path, case, warmup: int, steps: int, timeout: float = 600.0, env: dict | None = None,
+                stderr_out: list | None = None):
     """Run a harness binary over warmup + steps copies of one case; per-case seconds of the timed ones."""
     import cases
 
     with tempfile.TemporaryDirectory(prefix="nc_bench_") as tmp:
         root = Path(tmp)
         make_case_dir(root, case, warmup + steps)
-        r = subprocess.run([str(binary), str(root)], capture_output=True, text=True, timeout=timeout)
+        r = subprocess.run([str(binary), str(root)], capture_output=True, text=True, timeout=timeout,
+                           env=None if env is None else {**os.environ, **env})
+        if stderr_out is not None:
+            stderr_out.append(r.stderr)
         if r.returncode != 0:
             raise RuntimeError(f"{binary.name} exited {r.returncode}: {r.stderr[-400:]}")
         res = cases.read_results(root)
@@ -440,6 +444,10 @@ def ours(args) -> dict | None:
         if not np.array_equal(out, ref):
             raise RuntimeError("harness runner output differs from the library")
         per = statistics.mean(secs)
+        # a separate, shorter run with the library's host-path trace: where one call's time goes
+        traced: list = []
+        run_harness(RUNNER, case, 5, 20, env={"NC_TRACE": "1"}, stderr_out=traced)
+        phases = trace_phases(traced[0], 20)
         h2d_gbs, d2h_gbs = copy_rates(dev, 2 * N * L * 4, N * L * 4)
         h2d_ms = 2 * N * L * 4 / (h2d_gbs * 1e9) * 1e3
         d2h_ms = N * L * 4 / (d2h_gbs * 1e9) * 1e3
@@ -454,6 +462,7 @@ def ours(args) -> dict | None:
                                            "block needs residues of coefficients from the whole operand), and every "
                                            "output byte after it; copy rates measured here from pinned memory in the "
                                            "library's chunk sizes (4 MiB up, 2 MiB down), one direction at a time")},
+                         "phases_us": phases,
                          "calls": e2e_steps, "warmup_calls": e2e_warmup, "init_s": init_s,
                          "via": "fherma_run in the library's harness runner (pageable std::vector in/out); "
                                 "first_call_ms is the first call after fherma_init"}
@@ -478,7 +487,26 @@ def ours(args) -> dict | None:
     return result if rank == 0 else None
 
 
-def copy_rates(dev, up_bytes: int, down_bytes: int, reps: int = 5) -> tuple[float, float]:
+def trace_phases(stderr: str, last: int) -> dict | None:
+    """Median over the last `last` calls of each field of the library's NC_TRACE lines: device-clock
+    ends of a's upload, a's forward transform, b's upload, the product and the download, and host
+    times at which a and b were staged, everything was enqueued, and the result was copied out
+    (microseconds from the call's start)."""
+    rows = []
+    for line in stderr.splitlines():
+        if line.startswith("nc_trace "):
+            rows.append(dict((k, float(v)) for k, v in (f.split("=") for f in line.split()[1:])))
+    rows = rows[-last:]
+    if not rows:
+        return None
+    out = {k: round(statistics.median(r[k] for r in rows), 1) for k in rows[0]}
+    out["calls"] = len(rows)
+    out["what"] = ("device clock (a_uploaded .. downloaded) and host clock (a_staged .. collected), us from the "
+                   "call's start, median over calls of a separate traced run (NC_TRACE=1)")
+    return out
+
+
+def copy_rates(dev, up_bytes: int, down_bytes: int, reps: int = 20) -> tuple[float, float]:
     """GB/s of pinned host -> device copies of `up_bytes` in 4 MiB chunks and device -> pinned host
     copies of `down_bytes` in 2 MiB chunks (the host path's chunk sizes), best of `reps`."""
     import torch

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -292,6 +293,9 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int fac
         check(cudaStreamSynchronize(p->stream), "plan constants upload");
         check(cudaEventCreate(&p->ev_start), "event");
         check(cudaEventCreate(&p->ev_stop), "event");
+        if (const char* tr = std::getenv("NC_TRACE")) p->trace = tr[0] == '1';
+        if (p->trace)
+            for (auto& ev : p->ev_trace) check(cudaEventCreate(&ev), "event");
         for (auto& ev : p->ev_stage) check(cudaEventCreate(&ev), "event");
         device_self_test(p->device);
     } catch (...) {
@@ -440,6 +444,8 @@ void plan_destroy(Plan* p) {
     cudaFreeHost(p->h_c);
     if (p->ev_start) cudaEventDestroy(p->ev_start);
     if (p->ev_stop) cudaEventDestroy(p->ev_stop);
+    for (auto ev : p->ev_trace)
+        if (ev) cudaEventDestroy(ev);
     for (auto ev : p->ev_stage)
         if (ev) cudaEventDestroy(ev);
     if (p->stream) cudaStreamDestroy(p->stream);
@@ -560,6 +566,14 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
     }
     ProductDesc d = n == 2 ? p->desc(p->d_a, p->d_b, p->d_c) : p->desc_chain(dev_ops, p->d_c);
     int groups = 1;  // column groups of b's upload (pairs only)
+    const bool trace = p->trace && n == 2;
+    auto since = [p] {
+        return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - p->trace_t0).count();
+    };
+    if (trace) {
+        p->trace_t0 = std::chrono::steady_clock::now();
+        check(cudaEventRecord(p->ev_trace[0], p->stream), "event");
+    }
     for (int op = 0; op < n; ++op) {
         cudaStream_t stream = op == 0 ? p->stream : p->copy_stream;
         if (op == 1) {
@@ -579,7 +593,12 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
                 fa.b = nullptr;
                 fa.c = nullptr;
                 fa.hat_out = p->d_hat;
+                if (trace) {
+                    p->trace_host[0] = since();
+                    check(cudaEventRecord(p->ev_trace[1], p->stream), "event");
+                }
                 check(launch_product(fa, p->tables->view(), p->cfg, p->stream), "kernel launch");
+                if (trace) check(cudaEventRecord(p->ev_trace[2], p->stream), "event");
                 d.mode = kModeCachedA;
                 d.a = nullptr;
                 d.a_hat = p->d_hat;
@@ -589,7 +608,27 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
             }
             check(cudaStreamWaitEvent(p->copy_stream, p->ev_a, 0), "stream wait");
         }
-        const bool grouped = op == 1 && groups > 1;
+        if (op == 1 && groups > 1) {
+            // group g is columns [g N2 / G, (g + 1) N2 / G) of every row segment: the copy threads
+            // stage its N1 pieces, then one strided copy takes it up and its residue tiles follow on
+            // the plan's stream, so on a host whose staging is slower than the link b's transfer
+            // starts after a quarter of b is staged, not all of it
+            const int N1 = 1 << (p->logN - p->cfg.logN2);
+            const size_t N2 = size_t(1) << p->cfg.logN2, row = N2 * size_t(p->L) * 4;
+            const size_t width = row / size_t(groups);
+            for (int g = 0; g < groups; ++g) {
+                const size_t col = size_t(g) * width;
+                p->pool->run([&](int part, int parts) {
+                    for (int u = part; u < N1; u += parts)
+                        stage_copy(pins[op] + size_t(u) * row + col, srcs[op] + size_t(u) * row + col, width);
+                });
+                check(cudaMemcpy2DAsync(devs[op] + col, row, pins[op] + col, row, width, size_t(N1),
+                                        cudaMemcpyHostToDevice, stream),
+                      "operand copy");
+                check(cudaEventRecord(p->ev_grp[size_t(g)], stream), "event");
+            }
+            continue;
+        }
         for (const auto& ch : upload_chunks(bytes, op == 0)) {
             const size_t off = ch.first, len = ch.second;
             p->pool->run([&](int part, int parts) {
@@ -597,25 +636,15 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
                 slice(len, part, parts, &lo, &hi);
                 if (hi > lo) stage_copy(pins[op] + off + lo, srcs[op] + off + lo, hi - lo);
             });
-            if (!grouped)
-                check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, len, cudaMemcpyHostToDevice, stream),
-                      "operand copy");
-        }
-        if (grouped) {
-            // b is staged whole (while a transfers); group g is columns [g N2 / G, (g + 1) N2 / G) of
-            // every row segment, one strided copy, then its residue tiles on the plan's stream
-            const int logN1 = p->logN - p->cfg.logN2;
-            const size_t N2 = size_t(1) << p->cfg.logN2, row = N2 * size_t(p->L) * 4;
-            const size_t width = row / size_t(groups);
-            for (int g = 0; g < groups; ++g) {
-                check(cudaMemcpy2DAsync(devs[op] + size_t(g) * width, row, pins[op] + size_t(g) * width, row, width,
-                                        size_t(1) << logN1, cudaMemcpyHostToDevice, stream),
-                      "operand copy");
-                check(cudaEventRecord(p->ev_grp[size_t(g)], stream), "event");
-            }
+            check(cudaMemcpyAsync(devs[op] + off, pins[op] + off, len, cudaMemcpyHostToDevice, stream),
+                  "operand copy");
         }
     }
     check(cudaEventRecord(p->ev_b, p->copy_stream), "event");
+    if (trace) {
+        p->trace_host[1] = since();
+        check(cudaEventRecord(p->ev_trace[3], p->copy_stream), "event");
+    }
     if (groups > 1) {
         if (p->timing) check(cudaEventRecord(p->ev_stage[0], p->stream), "event");
         for (int g = 0; g < groups; ++g) {
@@ -629,6 +658,7 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
               "kernel launch");
     }
     check(cudaEventRecord(p->ev_stop, p->stream), "event");
+    if (trace) check(cudaEventRecord(p->ev_trace[4], p->stream), "event");
     const auto out = download_chunks(bytes);
     for (size_t j = 0; j < out.size(); ++j) {
         check(cudaMemcpyAsync(reinterpret_cast<char*>(p->h_c) + out[j].first,
@@ -636,6 +666,10 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
                               p->stream),
               "product copy");
         check(cudaEventRecord(p->ev_out[j], p->stream), "event");
+    }
+    if (trace) {
+        check(cudaEventRecord(p->ev_trace[5], p->stream), "event");
+        p->trace_host[2] = since();
     }
 }
 
@@ -689,6 +723,17 @@ void plan_collect_host(Plan* p, uint32_t* c) {
     check(cudaError_t(err.load()), "product");
     // the last output chunk's event is the last work of the product on the plan's stream
     cudaEventElapsedTime(&p->last_kernel_ms, p->ev_start, p->ev_stop);
+    if (p->trace) {
+        // one line per call: device-clock phase ends (from the call's start event) and host times
+        p->trace_host[3] = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - p->trace_t0).count();
+        float g[5] = {0, 0, 0, 0, 0};
+        for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&g[i], p->ev_trace[0], p->ev_trace[i + 1]);
+        std::fprintf(stderr,
+                     "nc_trace a_uploaded=%.1f a_forward=%.1f b_uploaded=%.1f product=%.1f downloaded=%.1f "
+                     "a_staged=%.1f b_staged=%.1f enqueued=%.1f collected=%.1f\n",
+                     1e3 * g[0], 1e3 * g[1], 1e3 * g[2], 1e3 * g[3], 1e3 * g[4], p->trace_host[0], p->trace_host[1],
+                     p->trace_host[2], p->trace_host[3]);
+    }
 }
 
 void plan_multiply_host(Plan* p, const uint32_t* a, const uint32_t* b, uint32_t* c) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdint>
 #include <functional>
@@ -112,6 +113,12 @@ struct Plan {
     bool res_tc = true;              // plain path: residue stage on the tensor cores
     bool timing = false;             // record per-stage events
     cudaEvent_t ev_stage[4] = {nullptr, nullptr, nullptr, nullptr};
+    // Host-path trace (NC_TRACE=1 in the environment when the plan is created): every host-buffer
+    // product writes one line to stderr with its phases in microseconds since the call began.
+    bool trace = false;
+    cudaEvent_t ev_trace[6] = {};  // call start, a uploaded, a forward, b uploaded, product, downloaded
+    double trace_host[4] = {0, 0, 0, 0};  // a staged, b staged, enqueued, collected (us)
+    std::chrono::steady_clock::time_point trace_t0;
 
     size_t limbs() const { return size_t(N) * size_t(L); }
     ProductDesc desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const;

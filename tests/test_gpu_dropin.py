@@ -16,6 +16,7 @@ Matches reference main.cpp:59-86 (init, timed run per case, c.bin per case, free
 from __future__ import annotations
 
 import hashlib
+import os
 import json
 import subprocess
 import sys
@@ -76,3 +77,23 @@ def test_contract_binary_on_the_bench_workload(gpu, name, tmp_path):
     want = oracle.negacyclic(c.N, c.q_limbs, c.a, c.b)
     for i, out in enumerate(_run(binary, c, tmp_path)):
         assert np.array_equal(out, want), f"call {i}: {int((out != want).any(axis=1).sum())} coefficients differ"
+
+
+def test_host_path_trace(gpu, tmp_path):
+    """NC_TRACE=1: one line per fherma_run with the call's phases in order (device clock for the
+    transfers and kernels, host clock for staging, enqueueing and the copy-out)."""
+    binary = _binary("library_runner")
+    c = cases.make_case(16384, 868, 77, edge_frac=0.01)
+    cases.write_case_dir(tmp_path, c.N, c.W, c.L, c.q, [(c.a, c.b)] * 3)
+    env = dict(os.environ, NC_TRACE="1")
+    r = subprocess.run([str(binary), str(tmp_path)], capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr[-1000:]
+    lines = [ln for ln in r.stderr.splitlines() if ln.startswith("nc_trace ")]
+    assert len(lines) == 3, r.stderr[-1000:]
+    for ln in lines:
+        f = dict((k, float(v)) for k, v in (x.split("=") for x in ln.split()[1:]))
+        assert 0 < f["a_uploaded"] <= f["a_forward"]
+        assert f["a_uploaded"] <= f["b_uploaded"] <= f["product"] <= f["downloaded"]
+        assert 0 < f["a_staged"] <= f["b_staged"] <= f["enqueued"] <= f["collected"]
+    want = oracle.negacyclic(c.N, c.q_limbs, c.a, c.b)
+    assert np.array_equal(cases.read_output(tmp_path, 2, c.N, c.L), want)
