@@ -34,7 +34,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", f"-I{INCLUDE}", f"-I{CSRC}"]
 
 LIB_SOURCES = ["hostmath.cpp", "k_dec.cu", "k_row.cu", "k_crt.cu", "k_batch.cu", "kernels.cu", "batch.cu",
-               "engine.cu", "server.cu", "api.cu", "noalloc.cu", "k_residues.cu", "k_crt_tc.cu", "k_dec_tc.cu"]
+               "engine.cu", "server.cu", "api.cu", "noalloc.cu", "k_residues.cu", "k_crt_tc.cu", "k_dec_tc.cu",
+               "k_w32.cu"]
 RUNNER_SOURCES = ["runner.cpp"]
 
 
@@ -83,7 +84,7 @@ def _compile(src: Path, verbose: bool) -> Path:
 
 # One translation unit of every library source, in dependency order.
 SOLVE_CU_SOURCES = ["hostmath.cpp", "kernels.cu", "k_dec.cu", "k_row.cu", "k_crt.cu", "k_dec_tc.cu", "k_crt_tc.cu",
-                    "k_batch.cu", "k_residues.cu", "batch.cu", "engine.cu", "server.cu", "api.cu", "noalloc.cu"]
+                    "k_w32.cu", "k_batch.cu", "k_residues.cu", "batch.cu", "engine.cu", "server.cu", "api.cu", "noalloc.cu"]
 
 SOLVE_CU_HEAD = """\
 // solve.cu: the B200 negacyclic product library (c = a*b mod (X^N + 1, q)) as one source file,

@@ -15,6 +15,7 @@
 #include "engine.h"
 #include "hostmath.h"
 #include "handles.h"
+#include "kernel_registry.h"
 #include "kernels.h"
 #include "server.h"
 
@@ -351,10 +352,47 @@ int nc_plan_set_row_config(nc_plan* plan, int log_block, int log_radix, int thre
 int nc_plan_get_row_config(const nc_plan* plan, int* log_block, int* log_radix, int* threads) {
     return guarded([&] {
         if (!plan) throw nc::Error(nc::kEInval, "null plan");
-        if (log_block) *log_block = plan->p->cfg.logN2;
-        if (log_radix) *log_radix = plan->p->cfg.logE;
-        if (threads) *threads = plan->p->cfg.threads;
+        const nc::RowConfig& c = plan->p->plain_cfg();
+        if (log_block) *log_block = c.logN2;
+        if (log_radix) *log_radix = c.logE;
+        if (threads) *threads = c.threads;
     });
+}
+
+int nc_row_variants32(uint32_t log_n, int* triples, int max_variants) {
+    if (log_n < 1 || log_n > uint32_t(nc::kMaxLogN) || (!triples && max_variants > 0)) {
+        g_last_error = "log_n must be 1..16";
+        return NC_EINVAL;
+    }
+    std::vector<nc::RowConfig> v;
+    for (const nc::RowConfig& c : nc::all_row32_variants())
+        if (nc::row_config_valid(int(log_n), c)) v.push_back(c);
+    int n = 0;
+    for (const auto& c : v) {
+        if (n >= max_variants) break;
+        triples[3 * n] = c.logN2;
+        triples[3 * n + 1] = c.logE;
+        triples[3 * n + 2] = c.threads;
+        ++n;
+    }
+    return max_variants <= 0 ? int(v.size()) : n;
+}
+
+int nc_plan_set_word_bits(nc_plan* plan, int bits) {
+    return guarded([&] {
+        if (!plan) throw nc::Error(nc::kEInval, "null plan");
+        nc::plan_set_word_bits(plan->p, bits);
+    });
+}
+
+int nc_plan_word_bits(const nc_plan* plan, uint32_t* k) {
+    if (!plan) {
+        g_last_error = "null plan";
+        return NC_EINVAL;
+    }
+    const bool w32 = plan->p->use_w32();
+    if (k) *k = uint32_t(w32 ? plan->p->k32 : plan->p->k);
+    return w32 ? 32 : 64;
 }
 
 int nc_plan_autotune(nc_plan* plan, int reps, float* best_ms) {

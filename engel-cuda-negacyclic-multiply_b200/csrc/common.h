@@ -73,6 +73,8 @@ struct QConst {
 };
 constexpr int kMqStride = kMaxL + 2;
 
+struct QConst32;
+
 // One negacyclic product as the kernels see it. All pointers are device pointers.
 struct ProductDesc {
     const uint32_t* a;      // N x L limbs (may be null when a_hat is given)
@@ -94,6 +96,34 @@ struct ProductDesc {
     const uint32_t* x_more[kMaxFactors - 2];  // further operands (N x L limbs)
     uint64_t* r_more[kMaxFactors - 2];        // their residues (k x N scratch)
     uint32_t res_tc;        // residue stage of the plain path on the tensor cores (k <= 32)
+    // Non-null: the 30-bit word engine runs this product (a pair; k counts its primes, and the
+    // residue buffers ra, rb, a_hat and hat_out hold k x N u32).
+    const QConst32* qc32;
+};
+
+// ------------------------------------------------------------------------------------------
+// The 30-bit word engine: primes p < 2^30 with p = 1 (mod 2^17), one u32 residue each.
+
+constexpr int kMaxPrimes32 = 64;         // 4 bytes of v_i x 64 primes = 256, the CRT contraction's K
+constexpr int kDecTc32PassPrimes = 32;   // residue MMAs: 4 byte planes x 32 primes = 128 columns
+
+// Per-prime constants of the 30-bit set.
+struct PrimeConst32 {
+    uint32_t p;
+    uint32_t pinv;  // -p^-1 mod 2^32 (Montgomery)
+    uint32_t bar;   // floor(2^50 / p): reduction of a 48-bit folded residue sum
+    uint32_t quo;   // floor(2^61 / p): the CRT quotient estimate
+};
+
+// Per-(q, N) constants of the 30-bit engine's CRT + Barrett stage.
+struct QConst32 {
+    uint32_t L, LW, k, qbits, logN, pad0;
+    uint32_t q[kMaxL + 2];
+    uint32_t neg_m[kMaxL + 2];             // (-M) mod q, M = prod of the k primes
+    uint32_t mu[4];                        // floor(2^(qbits + kBarrettT + 1) / q)
+    uint32_t y[kMaxPrimes32];              // (M/p_i)^-1 N^-1 2^32 mod p_i (2^32: the pointwise Montgomery factor)
+    uint32_t ys[kMaxPrimes32];             // floor(y 2^32 / p_i)
+    uint32_t mq[kMaxPrimes32 * (kMaxL + 2)];  // (M/p_i) mod q, row stride kMaxL + 2
 };
 
 // Operand f of a product (0: a, 1: b, 2..: x_more) and its residue buffer.
@@ -115,6 +145,12 @@ struct Tables {
     const uint64_t* pow32;    // [kMaxPrimes][kMaxL]: 2^(32 l) mod p_i
     const uint64_t* primes;   // [kMaxPrimes]
     const uint4* res_w;       // [kMaxPrimes][8 K chunks][8 byte planes][16 B]: byte c of 2^(8 b) mod p_i
+    // 30-bit engine
+    const uint2* fwd32;           // [kMaxPrimes32][kMaxN]: psi^bitrev16(j) and floor(w 2^32 / p)
+    const uint2* inv32;           // [kMaxPrimes32][kMaxN]: psi^-bitrev16(j) and its companion
+    const PrimeConst32* pc32;     // [kMaxPrimes32]
+    const uint32_t* pow32_32;     // [kMaxPrimes32][kMaxL]: 2^(32 l) mod p_i
+    const uint4* res_w32;         // [prime pairs][8 K chunks][8 rows: 4 byte planes of each][16 B]
 };
 
 // Dynamic shared memory of each stage.

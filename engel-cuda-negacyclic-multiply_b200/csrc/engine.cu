@@ -10,6 +10,7 @@
 
 #include "hostcopy.h"
 #include "hostmath.h"
+#include "kernel_registry.h"
 #include "kernels.h"
 
 namespace nc {
@@ -32,6 +33,45 @@ int current_device() {
 namespace {
 std::mutex g_tables_mu;
 std::map<int, DeviceTables*> g_tables;
+
+void free_tables(DeviceTables* t) {
+    for (void* ptr : {static_cast<void*>(t->fwd), static_cast<void*>(t->inv), static_cast<void*>(t->pow32),
+                      static_cast<void*>(t->primes), static_cast<void*>(t->res_w), static_cast<void*>(t->fwd32),
+                      static_cast<void*>(t->inv32), static_cast<void*>(t->pc32), static_cast<void*>(t->pow32_32),
+                      static_cast<void*>(t->res_w32)})
+        cudaFree(ptr);
+}
+
+// The 30-bit engine's tables: twiddles (w, floor(w 2^32 / p)), prime constants, 2^(32 l) mod p,
+// and the residue stage's weight bytes (byte c of 2^(8 b) mod p_i at
+// [i / 2][b / 16][4 (i % 2) + c][b % 16], b < 128: the MMA's B rows of a prime pair).
+void upload_tables32(DeviceTables* t) {
+    const HostTables32& h = host_tables32();
+    const size_t tw = size_t(kMaxPrimes32) * kMaxN * sizeof(uint2);
+    check(cudaMalloc(&t->fwd32, tw), "30-bit twiddle table");
+    check(cudaMalloc(&t->inv32, tw), "30-bit inverse twiddle table");
+    check(cudaMemcpy(t->fwd32, h.fwd.data(), tw, cudaMemcpyHostToDevice), "30-bit twiddle upload");
+    check(cudaMemcpy(t->inv32, h.inv.data(), tw, cudaMemcpyHostToDevice), "30-bit inverse twiddle upload");
+    check(cudaMalloc(&t->pc32, size_t(kMaxPrimes32) * sizeof(PrimeConst32)), "30-bit prime table");
+    check(cudaMemcpy(t->pc32, h.pc.data(), size_t(kMaxPrimes32) * sizeof(PrimeConst32), cudaMemcpyHostToDevice),
+          "30-bit prime upload");
+    check(cudaMalloc(&t->pow32_32, size_t(kMaxPrimes32) * kMaxL * 4), "30-bit limb weights");
+    check(cudaMemcpy(t->pow32_32, h.pow32.data(), size_t(kMaxPrimes32) * kMaxL * 4, cudaMemcpyHostToDevice),
+          "30-bit limb weight upload");
+    std::vector<uint8_t> w(size_t(kMaxPrimes32 / 2) * 1024, 0);
+    for (int i = 0; i < kMaxPrimes32; ++i) {
+        const uint64_t p = h.pc[size_t(i)].p;
+        uint64_t v = 1;
+        for (int b = 0; b < 128; ++b) {
+            for (int c = 0; c < 4; ++c)
+                w[size_t(i / 2) * 1024 + size_t(b / 16) * 128 + size_t(4 * (i % 2) + c) * 16 + size_t(b % 16)] =
+                    uint8_t(v >> (8 * c));
+            v = v * 256u % p;
+        }
+    }
+    check(cudaMalloc(&t->res_w32, w.size()), "30-bit residue weight table");
+    check(cudaMemcpy(t->res_w32, w.data(), w.size(), cudaMemcpyHostToDevice), "30-bit residue weight upload");
+}
 }  // namespace
 
 DeviceTables* acquire_tables(int device) {
@@ -79,17 +119,14 @@ DeviceTables* acquire_tables(int device) {
         }
         check(cudaMalloc(&t->res_w, w.size()), "residue weight table");
         check(cudaMemcpy(t->res_w, w.data(), w.size(), cudaMemcpyHostToDevice), "residue weight upload");
+        if (t->tensor_cores) upload_tables32(t);
         check(prepare_kernels(h.pc.data(), h.pow32.data()), "kernel preparation");
         check(prepare_noalloc(device), "allocation-free scratch set-up");
         // a synchronous copy from pageable memory may return before its last DMA lands, and the
         // kernels run on non-blocking streams that do not order after it: wait for the device
         check(cudaDeviceSynchronize(), "table upload");
     } catch (...) {
-        cudaFree(t->fwd);
-        cudaFree(t->inv);
-        cudaFree(t->pow32);
-        cudaFree(t->primes);
-        cudaFree(t->res_w);
+        free_tables(t);
         delete t;
         throw;
     }
@@ -106,17 +143,13 @@ void release_tables(DeviceTables* t) {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(t->device);
-    cudaFree(t->fwd);
-    cudaFree(t->inv);
-    cudaFree(t->pow32);
-    cudaFree(t->primes);
-    cudaFree(t->res_w);
+    free_tables(t);
     cudaSetDevice(prev);
     delete t;
 }
 
-// Host-side self-checks, once per process: known answers of the host arithmetic, the prime set,
-// and a sample of every prime's tables (psi, 2^(32 l) mod p, twiddles and Shoup companions).
+// Host-side self-checks, once per process: known answers of the host arithmetic, both prime
+// sets, and a sample of every prime's tables (psi, 2^(32 l) mod p, twiddles and Shoup companions).
 const std::string& host_self_check() {
     static std::string err;
     static std::once_flag once;
@@ -124,6 +157,8 @@ const std::string& host_self_check() {
         err = check_arithmetic();
         if (err.empty()) err = check_prime_set();
         if (err.empty()) err = check_tables(host_tables(), 64);
+        if (err.empty()) err = check_prime_set32();
+        if (err.empty()) err = check_tables32(host_tables32(), 64);
     });
     return err;
 }
@@ -202,6 +237,24 @@ ProductDesc Plan::desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const 
     return d;
 }
 
+ProductDesc Plan::desc_plain(const uint32_t* a, const uint32_t* b, uint32_t* c) const {
+    ProductDesc d = desc(a, b, c);
+    if (use_w32()) {
+        d.k = uint32_t(k32);
+        d.qc32 = d_qc32;
+        d.crt_b = d_crt_b32;
+        d.logN2 = uint32_t(cfg32.logN2);
+        d.res_tc = 1u;
+    }
+    return d;
+}
+
+size_t Plan::residue_bytes() const {
+    const size_t r64 = size_t(k) * size_t(N) * sizeof(uint64_t);
+    const size_t r32 = size_t(k32) * size_t(N) * sizeof(uint32_t);
+    return r64 > r32 ? r64 : r32;
+}
+
 ProductDesc Plan::desc_chain(const uint32_t* const* x, uint32_t* c) const {
     ProductDesc d = desc(x[0], x[1], c);
     d.factors = uint32_t(factors);
@@ -232,6 +285,38 @@ std::vector<uint8_t> crt_tc_table(const QConst& hq) {
                     uint8_t(word >> (8 * (byte % 4)));
             }
     return b;
+}
+
+// The same table for the 30-bit engine: K byte 4 i + a (a < 4) of output column c holds byte
+// c - a of (M/p_i) mod q.
+std::vector<uint8_t> crt_tc32_table(const QConst32& hq) {
+    const int LW = int(hq.LW), L = int(hq.L), k = int(hq.k);
+    const int NC = crt_tc_cols(LW);
+    std::vector<uint8_t> b(crt_tc_table_bytes(LW), 0);
+    for (int c = 0; c < NC; ++c)
+        for (int i = 0; i < k; ++i)
+            for (int a = 0; a < 4; ++a) {
+                const int byte = c - a;
+                if (byte < 0 || byte >= 4 * L) continue;
+                const uint32_t word = hq.mq[size_t(i) * kMqStride + size_t(byte / 4)];
+                const int K = 4 * i + a;
+                b[size_t(c / 8) * 2048 + size_t(K / 16) * 128 + size_t(c % 8) * 16 + size_t(K % 16)] =
+                    uint8_t(word >> (8 * (byte % 4)));
+            }
+    return b;
+}
+
+bool word64_forced() {
+    const char* word = std::getenv("NC_WORD_BITS");
+    return word && std::atoi(word) == 64;
+}
+
+// Row configuration of the 30-bit engine before any tuning: blocks of 2^11 with radix-8 passes
+// where N allows them, else the largest radix-16 block.
+RowConfig default_row_config32(int logN) {
+    RowConfig c{logN < 11 ? logN : 11, 3, 256};
+    if (!row_config_valid(logN, c) || !row32_kernel(c)) c = RowConfig{logN < kRowLogMax ? logN : kRowLogMax, 4, 256};
+    return c;
 }
 
 }  // namespace
@@ -274,6 +359,20 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int fac
     }
     p->k = int(p->hq.k);
     if (!tuned_row_config(logN, int(L), &p->cfg)) p->cfg = default_row_config(logN);
+    // the 30-bit engine: pairs whose bound fits its 64 primes
+    bool w32_consts = false;
+    if (factors == 2 && build_qconst32(q, int(L), logN, &p->hq32).empty()) {
+        const std::string e32 = check_qconst32(p->hq32);
+        if (!e32.empty()) {
+            delete p;
+            throw Error(kESelfCheck, "init self-check of the plan's 30-bit constants: " + e32);
+        }
+        w32_consts = true;
+        p->k32 = int(p->hq32.k);
+    }
+    p->cfg32 = default_row_config32(logN);
+    bool tuned_w32 = false;
+    const bool tuned = tuned_engine(logN, int(L), &p->cfg32, &tuned_w32);
     try {
         p->device = current_device();
         p->tables = acquire_tables(p->device);
@@ -289,6 +388,20 @@ Plan* plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int fac
             check(cudaMalloc(&p->d_crt_b, crt_b.size()), "CRT table");
             check(cudaMemcpyAsync(p->d_crt_b, crt_b.data(), crt_b.size(), cudaMemcpyHostToDevice, p->stream),
                   "CRT table upload");
+        }
+        std::vector<uint8_t> crt_b32;
+        if (w32_consts && p->tables->tensor_cores) {
+            check(cudaMalloc(&p->d_qc32, sizeof(QConst32)), "30-bit plan constants");
+            check(cudaMemcpyAsync(p->d_qc32, &p->hq32, sizeof(QConst32), cudaMemcpyHostToDevice, p->stream),
+                  "30-bit plan constants upload");
+            crt_b32 = crt_tc32_table(p->hq32);
+            check(cudaMalloc(&p->d_crt_b32, crt_b32.size()), "30-bit CRT table");
+            check(cudaMemcpyAsync(p->d_crt_b32, crt_b32.data(), crt_b32.size(), cudaMemcpyHostToDevice, p->stream),
+                  "30-bit CRT table upload");
+            p->w32_ok = true;
+            // NC_WORD_BITS=64 keeps the 62-bit engine; otherwise the engine an autotune of this
+            // (N, L) picked earlier in the process, else the 30-bit engine
+            p->w32 = !word64_forced() && (tuned ? tuned_w32 : true);
         }
         check(cudaStreamSynchronize(p->stream), "plan constants upload");
         check(cudaEventCreate(&p->ev_start), "event");
@@ -311,9 +424,9 @@ std::map<int, int> g_selftest;  // device -> 1 while its self-test runs, 2 once 
 }  // namespace
 
 // Once per device, before the first plan there is handed out: an N = 8 product modulo
-// q = 2^127 - 1 with 0, 1 and q - 1 among its coefficients, by the default stages (tensor-core
-// residues and CRT where the device has them) and by the integer-pipe stages, compared with the
-// host schoolbook. The plan it creates runs no self-test of its own.
+// q = 2^127 - 1 with 0, 1 and q - 1 among its coefficients, by the 30-bit engine and the 62-bit
+// tensor-core stages (where the device has tensor cores) and by the 62-bit integer-pipe stages,
+// compared with the host schoolbook. The plan it creates runs no self-test of its own.
 void device_self_test(int device) {
     {
         std::lock_guard<std::mutex> lock(g_selftest_mu);
@@ -349,15 +462,17 @@ void device_self_test(int device) {
         check(cudaMalloc(&d, size_t(3) * N * L * 4), "self-test buffers");
         check(cudaMemcpy(d, a.data(), size_t(N) * L * 4, cudaMemcpyHostToDevice), "self-test upload");
         check(cudaMemcpy(d + N * L, b.data(), size_t(N) * L * 4, cudaMemcpyHostToDevice), "self-test upload");
-        for (int engines = 0; engines < 2 && err.empty(); ++engines) {
-            if (engines == 1) p->res_tc = p->crt_tc = false;
+        // engines: the 30-bit one (where the device has it), the 62-bit tensor-core stages, the
+        // 62-bit integer-pipe stages
+        const char* names[3] = {"30-bit", "default 62-bit", "integer-pipe 62-bit"};
+        for (int engines = p->w32_ok ? 0 : 1; engines < 3 && err.empty(); ++engines) {
+            p->w32 = engines == 0;
+            if (engines == 2) p->res_tc = p->crt_tc = false;
             check(cudaMemsetAsync(d + 2 * N * L, 0xff, size_t(N) * L * 4, p->stream), "self-test output");
             plan_multiply_device(p, d, d + N * L, d + 2 * N * L, p->stream);
             check(cudaStreamSynchronize(p->stream), "self-test product");
             check(cudaMemcpy(got.data(), d + 2 * N * L, size_t(N) * L * 4, cudaMemcpyDeviceToHost), "self-test download");
-            if (got != want)
-                err = engines == 0 ? "the default stages' N = 8 product differs from the schoolbook"
-                                   : "the integer-pipe stages' N = 8 product differs from the schoolbook";
+            if (got != want) err = std::string("the ") + names[engines] + " stages' N = 8 product differs from the schoolbook";
         }
     } catch (...) {
         cudaFree(d);
@@ -373,11 +488,12 @@ void device_self_test(int device) {
     if (!err.empty()) throw Error(kESelfCheck, "device self-test: " + err);
 }
 
-// The plain path's residue scratch (2 k N u64), allocated on its first use: plans used only
-// inside batches or through the allocation-free entry point never hold it.
+// The plain path's residue scratch (k N u64 or k32 N u32 per operand, whichever is larger),
+// allocated on its first use: plans used only inside batches or through the allocation-free
+// entry point never hold it.
 void ensure_scratch(Plan* p) {
     if (p->d_ra) return;
-    const size_t res = size_t(p->k) * p->N * sizeof(uint64_t);
+    const size_t res = p->residue_bytes();
     uint64_t* bufs[kMaxFactors] = {};
     for (int f = 0; f < p->factors; ++f) {
         const cudaError_t e = cudaMalloc(&bufs[f], res);
@@ -402,7 +518,7 @@ void ensure_host_path(Plan* p) {
     check(cudaMallocHost(&p->h_a, limbs), "pinned a");
     check(cudaMallocHost(&p->h_b, limbs), "pinned b");
     check(cudaMallocHost(&p->h_c, limbs), "pinned c");
-    check(cudaMalloc(&p->d_hat, size_t(p->k) * p->N * sizeof(uint64_t)), "operand a in the NTT domain");
+    check(cudaMalloc(&p->d_hat, p->residue_bytes()), "operand a in the NTT domain");
     for (int f = 2; f < p->factors; ++f) {
         check(cudaMalloc(&p->d_x[f - 2], limbs), "input operand");
         check(cudaMallocHost(&p->h_x[f - 2], limbs), "pinned operand");
@@ -428,6 +544,8 @@ void plan_destroy(Plan* p) {
     if (p->ev_b) cudaEventDestroy(p->ev_b);
     cudaFree(p->d_qc);
     cudaFree(p->d_crt_b);
+    cudaFree(p->d_qc32);
+    cudaFree(p->d_crt_b32);
     cudaFree(p->d_ra);
     cudaFree(p->d_rb);
     cudaFree(p->d_hat);
@@ -464,8 +582,8 @@ void plan_multiply_device(Plan* p, const uint32_t* d_a, const uint32_t* d_b, uin
          15) != 0)
         throw Error(kEInval, "device buffers must be 16-byte aligned");
     ensure_scratch(p);
-    const ProductDesc d = p->desc(d_a, d_b, d_c);
-    check(launch_product(d, p->tables->view(), p->cfg, stream, p->timing ? p->ev_stage : nullptr),
+    const ProductDesc d = p->desc_plain(d_a, d_b, d_c);
+    check(launch_product(d, p->tables->view(), p->plain_cfg(), stream, p->timing ? p->ev_stage : nullptr),
           "kernel launch");
 }
 
@@ -535,7 +653,7 @@ std::vector<std::pair<size_t, size_t>> download_chunks(size_t bytes) {
 int upload_groups(const Plan* p, const ProductDesc& d) {
     constexpr int kGroups = 4;
     if (p->N < (1 << 13)) return 1;
-    return residue_tiles(d, p->cfg) % kGroups == 0 ? kGroups : 1;
+    return residue_tiles(d, p->plain_cfg()) % kGroups == 0 ? kGroups : 1;
 }
 
 }  // namespace
@@ -564,7 +682,7 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
         pins[f] = reinterpret_cast<char*>(pin);
         devs[f] = reinterpret_cast<char*>(dev_ops[f]);
     }
-    ProductDesc d = n == 2 ? p->desc(p->d_a, p->d_b, p->d_c) : p->desc_chain(dev_ops, p->d_c);
+    ProductDesc d = n == 2 ? p->desc_plain(p->d_a, p->d_b, p->d_c) : p->desc_chain(dev_ops, p->d_c);
     int groups = 1;  // column groups of b's upload (pairs only)
     const bool trace = p->trace && n == 2;
     auto since = [p] {
@@ -597,14 +715,14 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
                     p->trace_host[0] = since();
                     check(cudaEventRecord(p->ev_trace[1], p->stream), "event");
                 }
-                check(launch_product(fa, p->tables->view(), p->cfg, p->stream), "kernel launch");
+                check(launch_product(fa, p->tables->view(), p->plain_cfg(), p->stream), "kernel launch");
                 if (trace) check(cudaEventRecord(p->ev_trace[2], p->stream), "event");
                 d.mode = kModeCachedA;
                 d.a = nullptr;
                 d.a_hat = p->d_hat;
                 groups = upload_groups(p, d);
             } else {
-                check(launch_residues(d, p->tables->view(), p->cfg, p->stream, 0, 1), "kernel launch");
+                check(launch_residues(d, p->tables->view(), p->plain_cfg(), p->stream, 0, 1), "kernel launch");
             }
             check(cudaStreamWaitEvent(p->copy_stream, p->ev_a, 0), "stream wait");
         }
@@ -613,8 +731,8 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
             // stage its N1 pieces, then one strided copy takes it up and its residue tiles follow on
             // the plan's stream, so on a host whose staging is slower than the link b's transfer
             // starts after a quarter of b is staged, not all of it
-            const int N1 = 1 << (p->logN - p->cfg.logN2);
-            const size_t N2 = size_t(1) << p->cfg.logN2, row = N2 * size_t(p->L) * 4;
+            const int N1 = 1 << (p->logN - p->plain_cfg().logN2);
+            const size_t N2 = size_t(1) << p->plain_cfg().logN2, row = N2 * size_t(p->L) * 4;
             const size_t width = row / size_t(groups);
             for (int g = 0; g < groups; ++g) {
                 const size_t col = size_t(g) * width;
@@ -649,12 +767,12 @@ void submit_host_operands(Plan* p, const uint32_t* const* x, int n) {
         if (p->timing) check(cudaEventRecord(p->ev_stage[0], p->stream), "event");
         for (int g = 0; g < groups; ++g) {
             check(cudaStreamWaitEvent(p->stream, p->ev_grp[size_t(g)], 0), "stream wait");
-            check(launch_residues(d, p->tables->view(), p->cfg, p->stream, 1, 1, g, groups), "kernel launch");
+            check(launch_residues(d, p->tables->view(), p->plain_cfg(), p->stream, 1, 1, g, groups), "kernel launch");
         }
         cudaEvent_t* ev = p->timing ? p->ev_stage : nullptr;
-        check(launch_product(d, p->tables->view(), p->cfg, p->stream, ev, nullptr, true), "kernel launch");
+        check(launch_product(d, p->tables->view(), p->plain_cfg(), p->stream, ev, nullptr, true), "kernel launch");
     } else {
-        check(launch_product(d, p->tables->view(), p->cfg, p->stream, p->timing ? p->ev_stage : nullptr, p->ev_b),
+        check(launch_product(d, p->tables->view(), p->plain_cfg(), p->stream, p->timing ? p->ev_stage : nullptr, p->ev_b),
               "kernel launch");
     }
     check(cudaEventRecord(p->ev_stop, p->stream), "event");
@@ -767,7 +885,12 @@ void plan_multiply_chain_device(Plan* p, const uint32_t* const* d_x, uint32_t* d
 
 namespace {
 std::mutex g_tune_mu;
-std::map<std::pair<int, int>, RowConfig> g_tuned;
+std::map<std::pair<int, int>, RowConfig> g_tuned;  // the 62-bit engine's row configuration
+struct Tuned32 {
+    RowConfig cfg;  // the 30-bit engine's row configuration
+    bool use;       // it was the faster engine
+};
+std::map<std::pair<int, int>, Tuned32> g_tuned32;
 }  // namespace
 
 bool tuned_row_config(int logN, int L, RowConfig* out) {
@@ -778,11 +901,40 @@ bool tuned_row_config(int logN, int L, RowConfig* out) {
     return true;
 }
 
+bool tuned_engine(int logN, int L, RowConfig* cfg32, bool* use_w32) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned32.find({logN, L});
+    if (it == g_tuned32.end()) return false;
+    *cfg32 = it->second.cfg;
+    *use_w32 = it->second.use;
+    return true;
+}
+
 void plan_set_row_config(Plan* p, const RowConfig& c) {
     if (!p) throw Error(kEInval, "null plan");
+    if (p->use_w32()) {
+        if (!row_config_valid(p->logN, c) || !row32_kernel(c))
+            throw Error(kEInval, "no compiled 30-bit row kernel for this configuration and N");
+        p->cfg32 = c;
+        return;
+    }
     if (!row_config_valid(p->logN, c) || !row_variant_exists(c))
         throw Error(kEInval, "no compiled row kernel for this configuration and N");
     p->cfg = c;
+}
+
+void plan_set_word_bits(Plan* p, int bits) {
+    if (!p) throw Error(kEInval, "null plan");
+    if (bits == 64) {
+        p->w32 = false;
+        return;
+    }
+    if (bits != 32) throw Error(kEInval, "word bits must be 32 or 64");
+    if (!p->w32_ok)
+        throw Error(kEInval,
+                    "the 30-bit engine needs tensor cores, a product of two operands and a bound within 64 primes "
+                    "below 2^30");
+    p->w32 = true;
 }
 
 float plan_autotune(Plan* p, int reps) {
@@ -804,12 +956,8 @@ float plan_autotune(Plan* p, int reps) {
     check(cudaMemcpyAsync(p->d_a, host.data(), words * 4, cudaMemcpyHostToDevice, p->stream), "tune upload");
     check(cudaMemcpyAsync(p->d_b, host.data(), words * 4, cudaMemcpyHostToDevice, p->stream), "tune upload");
     check(cudaStreamSynchronize(p->stream), "tune upload");
-    const RowConfig saved = p->cfg;
-    RowConfig best = saved;
-    float best_ms = 1e30f;
-    for (const RowConfig& c : row_variants(p->logN)) {
-        p->cfg = c;
-        const ProductDesc d = p->desc(p->d_a, p->d_b, p->d_c);
+    auto time_product = [&](const RowConfig& c) {
+        const ProductDesc d = p->desc_plain(p->d_a, p->d_b, p->d_c);
         check(launch_product(d, p->tables->view(), c, p->stream), "tune launch");  // warm-up
         check(cudaEventRecord(p->ev_start, p->stream), "event");
         for (int r = 0; r < reps; ++r) check(launch_product(d, p->tables->view(), c, p->stream), "tune launch");
@@ -817,16 +965,46 @@ float plan_autotune(Plan* p, int reps) {
         check(cudaEventSynchronize(p->ev_stop), "tune");
         float ms = 0.f;
         check(cudaEventElapsedTime(&ms, p->ev_start, p->ev_stop), "event");
-        ms /= float(reps);
+        return ms / float(reps);
+    };
+    // the 62-bit engine's row configurations
+    const bool was_w32 = p->w32;
+    p->w32 = false;
+    RowConfig best = p->cfg;
+    float best_ms = 1e30f;
+    for (const RowConfig& c : row_variants(p->logN)) {
+        p->cfg = c;
+        const float ms = time_product(c);
         if (ms < best_ms) {
             best_ms = ms;
             best = c;
         }
     }
     p->cfg = best;
+    // the 30-bit engine's, where it can run; the faster engine is kept
+    const bool try32 = p->w32_ok && p->res_tc && p->crt_tc && !word64_forced();
+    RowConfig best32 = p->cfg32;
+    float best32_ms = 1e30f;
+    if (try32) {
+        p->w32 = true;
+        for (const RowConfig& c : all_row32_variants()) {
+            if (!row_config_valid(p->logN, c)) continue;
+            p->cfg32 = c;
+            const float ms = time_product(c);
+            if (ms < best32_ms) {
+                best32_ms = ms;
+                best32 = c;
+            }
+        }
+        p->cfg32 = best32;
+        p->w32 = best32_ms < best_ms;
+    } else {
+        p->w32 = was_w32;
+    }
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tuned[{p->logN, p->L}] = best;
-    return best_ms;
+    if (try32) g_tuned32[{p->logN, p->L}] = Tuned32{best32, p->w32};
+    return try32 && best32_ms < best_ms ? best32_ms : best_ms;
 }
 
 }  // namespace nc

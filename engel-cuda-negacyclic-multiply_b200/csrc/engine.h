@@ -39,7 +39,13 @@ struct DeviceTables {
     uint64_t* primes = nullptr;  // [kMaxPrimes]
     uint4* res_w = nullptr;      // weight bytes of the tensor-core residue stage
     bool tensor_cores = false;   // compute capability 10.0: the sm_100a tcgen05 kernels run here
-    Tables view() const { return Tables{fwd, inv, pow32, primes, res_w}; }
+    // the 30-bit word engine's tables (about 75 MB; only on devices with tensor cores)
+    uint2* fwd32 = nullptr;
+    uint2* inv32 = nullptr;
+    PrimeConst32* pc32 = nullptr;
+    uint32_t* pow32_32 = nullptr;
+    uint4* res_w32 = nullptr;
+    Tables view() const { return Tables{fwd, inv, pow32, primes, res_w, fwd32, inv32, pc32, pow32_32, res_w32}; }
 };
 
 // Known answers of the host arithmetic, the prime set and sampled tables, checked once per
@@ -111,6 +117,16 @@ struct Plan {
     uint4* d_crt_b = nullptr;        // byte table of the tensor-core CRT (k <= 32), built at creation
     bool crt_tc = true;              // plain path: CRT accumulation on the tensor cores when available
     bool res_tc = true;              // plain path: residue stage on the tensor cores
+    // The 30-bit word engine for the plain path of a pair (k32 primes below 2^30): available with
+    // tensor cores when the bound fits 64 primes; in use while `w32` is set and both tensor-core
+    // stages are selected. Batches, chains and the allocation-free entry run the 62-bit engine.
+    bool w32_ok = false;
+    bool w32 = false;
+    int k32 = 0;
+    QConst32 hq32{};
+    QConst32* d_qc32 = nullptr;
+    uint4* d_crt_b32 = nullptr;
+    RowConfig cfg32{};               // row-stage tiling of the 30-bit engine
     bool timing = false;             // record per-stage events
     cudaEvent_t ev_stage[4] = {nullptr, nullptr, nullptr, nullptr};
     // Host-path trace (NC_TRACE=1 in the environment when the plan is created): every host-buffer
@@ -121,6 +137,13 @@ struct Plan {
     std::chrono::steady_clock::time_point trace_t0;
 
     size_t limbs() const { return size_t(N) * size_t(L); }
+    bool use_w32() const { return w32 && w32_ok && res_tc && crt_tc; }
+    // Row configuration and descriptor of the plain path's engine.
+    const RowConfig& plain_cfg() const { return use_w32() ? cfg32 : cfg; }
+    ProductDesc desc_plain(const uint32_t* a, const uint32_t* b, uint32_t* c) const;
+    // Bytes of one operand's residue scratch (either engine).
+    size_t residue_bytes() const;
+    // The 62-bit engine's descriptor.
     ProductDesc desc(const uint32_t* a, const uint32_t* b, uint32_t* c) const;
     // All `factors` operands of a chained product (device pointers).
     ProductDesc desc_chain(const uint32_t* const* x, uint32_t* c) const;
@@ -163,5 +186,10 @@ float plan_autotune(Plan* p, int reps);
 
 // The remembered choice for (logN, L), if any autotune ran in this process.
 bool tuned_row_config(int logN, int L, RowConfig* out);
+// The 30-bit engine's remembered row configuration for (logN, L) and whether it was the faster.
+bool tuned_engine(int logN, int L, RowConfig* cfg32, bool* use_w32);
+
+// The plain path's engine: 32 (the 30-bit word engine; throws if the plan cannot run it) or 64.
+void plan_set_word_bits(Plan* p, int bits);
 
 }  // namespace nc

@@ -456,4 +456,219 @@ std::string build_qconst(const uint32_t* q, int L, int logN, QConst* out, int fa
     return std::string();
 }
 
+// ---------------------------------------------------------------------------- 30-bit engine
+
+namespace {
+
+// The 64 largest primes below 2^30 that are 1 mod 2^17 (all above 2^29.8), descending.
+std::vector<PrimeConst32> make_prime_set32() {
+    std::vector<PrimeConst32> out;
+    const uint64_t step = 1ull << kRootLog;
+    for (uint64_t cand = (1ull << 30) - step + 1; int(out.size()) < kMaxPrimes32; cand -= step) {
+        if (!is_prime64(cand)) continue;
+        uint32_t inv = 1;  // p^-1 mod 2^32 by Newton's iteration (each step doubles the correct bits)
+        for (int it = 0; it < 5; ++it) inv *= 2u - uint32_t(cand) * inv;
+        PrimeConst32 c{};
+        c.p = uint32_t(cand);
+        c.pinv = 0u - inv;
+        c.bar = uint32_t((1ull << 50) / cand);
+        c.quo = uint32_t((1ull << 61) / cand);
+        out.push_back(c);
+    }
+    return out;
+}
+
+uint32_t shoup32(uint32_t w, uint32_t p) { return uint32_t((uint64_t(w) << 32) / p); }
+
+}  // namespace
+
+const std::vector<PrimeConst32>& prime_set32() {
+    static const std::vector<PrimeConst32> set = make_prime_set32();
+    return set;
+}
+
+int primes_needed32(int logN, int qbits) {
+    const int bound_bits = logN + 2 * qbits + 4;
+    Big prod{1};
+    const auto& ps = prime_set32();
+    for (int k = 1; k <= kMaxPrimes32; ++k) {
+        prod = mul_u64(prod, ps[size_t(k) - 1].p);
+        if (bits_of(prod) >= bound_bits) return k;
+    }
+    return -1;
+}
+
+const HostTables32& host_tables32() {
+    static HostTables32 t;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        t.pc = prime_set32();
+        t.psi.assign(kMaxPrimes32, 0);
+        t.pow32.assign(size_t(kMaxPrimes32) * kMaxL, 0);
+        t.fwd.assign(size_t(kMaxPrimes32) * kMaxN * 2, 0);
+        t.inv.assign(size_t(kMaxPrimes32) * kMaxN * 2, 0);
+        auto work = [](int i) {
+            const uint64_t p = t.pc[size_t(i)].p;
+            uint64_t psi = 0;
+            for (uint64_t g = 2; g < 1000000; ++g) {
+                const uint64_t c = powmod64(g, (p - 1) >> kRootLog, p);
+                if (powmod64(c, 1ull << kMaxLogN, p) == p - 1) {
+                    psi = c;
+                    break;
+                }
+            }
+            t.psi[size_t(i)] = uint32_t(psi);
+            uint64_t place = 1;
+            for (int l = 0; l < kMaxL; ++l) {
+                t.pow32[size_t(i) * kMaxL + size_t(l)] = uint32_t(place);
+                place = (place << 32) % p;
+            }
+            std::vector<uint32_t> pw(kMaxN + 1);
+            pw[0] = 1;
+            for (int e = 1; e <= kMaxN; ++e) pw[size_t(e)] = uint32_t(uint64_t(pw[size_t(e) - 1]) * psi % p);
+            uint32_t* f = t.fwd.data() + size_t(i) * kMaxN * 2;
+            uint32_t* g = t.inv.data() + size_t(i) * kMaxN * 2;
+            for (uint32_t j = 0; j < uint32_t(kMaxN); ++j) {
+                const uint32_t e = bitrev(j, kMaxLogN);
+                const uint32_t w = pw[e];
+                const uint32_t wi = e == 0 ? 1u : uint32_t(p - pw[size_t(kMaxN) - e]);  // psi^-e = -psi^(N - e)
+                f[2 * j] = w;
+                f[2 * j + 1] = shoup32(w, uint32_t(p));
+                g[2 * j] = wi;
+                g[2 * j + 1] = shoup32(wi, uint32_t(p));
+            }
+        };
+        const int nthreads = std::max(1, std::min<int>(16, int(std::thread::hardware_concurrency())));
+        std::vector<std::thread> pool;
+        for (int w = 0; w < nthreads; ++w)
+            pool.emplace_back([&, w] {
+                for (int i = w; i < kMaxPrimes32; i += nthreads) work(i);
+            });
+        for (auto& th : pool) th.join();
+    });
+    return t;
+}
+
+std::string check_prime_set32() {
+    const auto& ps = prime_set32();
+    if (int(ps.size()) != kMaxPrimes32) return "30-bit prime set size";
+    for (int i = 0; i < kMaxPrimes32; ++i) {
+        const PrimeConst32& c = ps[size_t(i)];
+        const std::string at = "30-bit prime " + std::to_string(i) + ": ";
+        if (!is_prime64(c.p)) return at + "composite";
+        if (((c.p - 1) & ((1u << kRootLog) - 1)) != 0) return at + "not 1 mod 2^17";
+        if (c.p >= (1u << 30) || c.p <= (1u << 29)) return at + "not in (2^29, 2^30)";
+        if (uint32_t(c.p * (0u - c.pinv)) != 1u) return at + "pinv is not -p^-1 mod 2^32";
+        if (uint64_t(c.bar) != (1ull << 50) / c.p || uint64_t(c.quo) != (1ull << 61) / c.p)
+            return at + "reciprocal constants";
+        if (i > 0 && c.p >= ps[size_t(i) - 1].p) return "30-bit prime set not descending";
+    }
+    return std::string();
+}
+
+std::string check_tables32(const HostTables32& t, int samples) {
+    for (int i = 0; i < kMaxPrimes32; ++i) {
+        const uint64_t p = t.pc[size_t(i)].p;
+        const uint64_t psi = t.psi[size_t(i)];
+        const std::string at = "30-bit prime " + std::to_string(i) + ": ";
+        if (powmod64(psi, 1ull << kMaxLogN, p) != p - 1) return at + "psi^(2^16) != -1";
+        for (int l = 0; l < kMaxL; ++l)
+            if (t.pow32[size_t(i) * kMaxL + size_t(l)] != powmod64(2, 32ull * uint64_t(l), p))
+                return at + "2^(32 l) mod p";
+        const uint32_t* f = t.fwd.data() + size_t(i) * kMaxN * 2;
+        const uint32_t* g = t.inv.data() + size_t(i) * kMaxN * 2;
+        for (int s = 0; s < samples; ++s) {
+            const uint32_t j = uint32_t((uint64_t(s) * 2654435761u + uint64_t(i)) % uint64_t(kMaxN));
+            const uint32_t e = bitrev(j, kMaxLogN);
+            if (f[2 * j] != powmod64(psi, e, p)) return at + "twiddle psi^bitrev(j)";
+            if (uint64_t(f[2 * j]) * g[2 * j] % p != 1) return at + "inverse twiddle";
+            for (const uint32_t* w : {f + 2 * j, g + 2 * j}) {
+                const uint64_t lhs = uint64_t(w[0]) << 32, qp = uint64_t(w[1]) * p;  // w' = floor(w 2^32 / p)
+                if (w[0] >= p || qp > lhs || lhs - qp >= p) return at + "Shoup companion of a twiddle";
+            }
+        }
+    }
+    return std::string();
+}
+
+std::string build_qconst32(const uint32_t* q, int L, int logN, QConst32* out) {
+    if (L < 1 || L > kMaxL) return "L must be between 1 and 32";
+    if (logN < 1 || logN > kMaxLogN) return "N must be a power of two from 2 to 65536";
+    if ((q[0] & 1u) == 0) return "q must be odd";
+    const int qbits = bit_length(q, L);
+    if (qbits <= 32 * (L - 1)) return "the top limb of q must be nonzero";
+    const int k = primes_needed32(logN, qbits);
+    if (k < 0) return "the coefficient bound does not fit the 64-prime 30-bit residue budget";
+    const auto& ps = prime_set32();
+    *out = QConst32{};
+    out->L = uint32_t(L);
+    out->LW = uint32_t((L + 1) & ~1);
+    out->k = uint32_t(k);
+    out->qbits = uint32_t(qbits);
+    out->logN = uint32_t(logN);
+    Big qb(q, q + L);
+    trim(qb);
+    for (int l = 0; l < L; ++l) out->q[l] = q[l];
+    Big M{1};
+    for (int i = 0; i < k; ++i) M = mul_u64(M, ps[size_t(i)].p);
+    const uint64_t N = 1ull << logN;
+    for (int i = 0; i < k; ++i) {
+        const uint64_t p = ps[size_t(i)].p;
+        const Big Mi = div_u64(M, p, nullptr);
+        uint64_t mi_mod_p = 0;
+        div_u64(Mi, p, &mi_mod_p);
+        // y = (M/p_i)^-1 N^-1 2^32 mod p_i: the 2^32 cancels the 2^-32 of the pointwise product
+        const uint64_t y = mulmod64(mulmod64(powmod64(mi_mod_p, p - 2, p), powmod64(N % p, p - 2, p), p),
+                                    (1ull << 32) % p, p);
+        out->y[i] = uint32_t(y);
+        out->ys[i] = shoup32(uint32_t(y), uint32_t(p));
+        const Big miq = divmod(Mi, qb, nullptr);
+        for (size_t l = 0; l < miq.size() && l < size_t(kMqStride); ++l) out->mq[size_t(i) * kMqStride + l] = miq[l];
+    }
+    const Big mmq = divmod(M, qb, nullptr);
+    Big neg = qb;
+    if (!mmq.empty()) sub_shifted(neg, mmq, 0);
+    else neg.clear();
+    if (cmp_big(neg, qb) == 0) neg.clear();
+    for (size_t l = 0; l < neg.size(); ++l) out->neg_m[l] = neg[l];
+    Big mu;
+    divmod(pow2(qbits + kBarrettT + 1), qb, &mu);
+    if (bits_of(mu) > 96) return "internal: Barrett constant too wide";
+    for (size_t l = 0; l < mu.size() && l < 4; ++l) out->mu[l] = mu[l];
+    return std::string();
+}
+
+std::string check_qconst32(const QConst32& c) {
+    const int k = int(c.k), L = int(c.L);
+    const auto& ps = prime_set32();
+    if (k < 1 || k > kMaxPrimes32 || L < 1 || L > kMaxL) return "prime or limb count";
+    Big qb(c.q, c.q + L);
+    trim(qb);
+    if (bits_of(qb) != int(c.qbits)) return "bit length of q";
+    Big neg(c.neg_m, c.neg_m + kMqStride);
+    trim(neg);
+    if (cmp_big(neg, qb) >= 0) return "(-M) mod q is not below q";
+    const uint64_t N = 1ull << c.logN;
+    for (int i = 0; i < k; ++i) {
+        const uint64_t p = ps[size_t(i)].p;
+        const std::string at = "30-bit prime " + std::to_string(i) + ": ";
+        uint64_t mi = 1;
+        for (int j = 0; j < k; ++j)
+            if (j != i) mi = mulmod64(mi, ps[size_t(j)].p % p, p);
+        // y_i (M / p_i) N = 2^32 (mod p_i)
+        if (mulmod64(mulmod64(c.y[i], mi, p), N % p, p) != (1ull << 32) % p) return at + "y_i (M/p_i) N != 2^32";
+        const uint64_t lhs = uint64_t(c.y[i]) << 32, qp = uint64_t(c.ys[i]) * p;
+        if (c.y[i] >= p || qp > lhs || lhs - qp >= p) return at + "Shoup companion of y_i";
+        Big mq(c.mq + size_t(i) * kMqStride, c.mq + size_t(i) * kMqStride + kMqStride);
+        trim(mq);
+        if (cmp_big(mq, qb) >= 0) return at + "(M/p_i) mod q is not below q";
+        if (!divmod(add_big(mul_u64(mq, p), neg), qb, nullptr).empty()) return at + "(M/p_i mod q) p_i != M mod q";
+    }
+    Big mu(c.mu, c.mu + 4);
+    trim(mu);
+    const Big e = pow2(int(c.qbits) + kBarrettT + 1);
+    if (cmp_big(mul_big(mu, qb), e) > 0 || cmp_big(add_big(mul_big(mu, qb), qb), e) <= 0) return "Barrett constant mu";
+    return std::string();
+}
+
 }  // namespace nc

@@ -45,6 +45,30 @@ std::string check_prime_set();                               // primes, their 2^
 std::string check_tables(const HostTables& t, int samples);  // psi, 2^(32 l) mod p, sampled twiddles
 std::string check_qconst(const QConst& c);                   // CRT identities and mu of one plan
 
+// ------------------------------------------------------------------ the 30-bit word engine
+
+struct HostTables32 {
+    std::vector<PrimeConst32> pc;  // kMaxPrimes32, descending below 2^30
+    std::vector<uint32_t> psi;     // primitive 2^17-th root of unity per prime
+    std::vector<uint32_t> pow32;   // kMaxPrimes32 * kMaxL: 2^(32 l) mod p
+    std::vector<uint32_t> fwd;     // kMaxPrimes32 * kMaxN * 2 (w, floor(w 2^32 / p))
+    std::vector<uint32_t> inv;     // same for psi^-1
+};
+
+// Built once per process (thread-safe); about 33 MB of host memory.
+const HostTables32& host_tables32();
+const std::vector<PrimeConst32>& prime_set32();
+
+// Primes of the 30-bit set for the bound of primes_needed (pairs only); -1 if more than 64.
+int primes_needed32(int logN, int qbits);
+
+// The 30-bit engine's CRT + Barrett constants. Returns an empty string or an error message.
+std::string build_qconst32(const uint32_t* q, int L, int logN, QConst32* out);
+
+std::string check_prime_set32();                                 // primes, 1 mod 2^17, constants
+std::string check_tables32(const HostTables32& t, int samples);  // psi, 2^(32 l) mod p, twiddles
+std::string check_qconst32(const QConst32& c);                   // CRT identities and mu
+
 // c = a * b mod (X^N + 1, q) by the schoolbook sum on big integers (small N only: the device
 // self-test's expected answer).
 void schoolbook_negacyclic(int N, int L, const uint32_t* q, const uint32_t* a, const uint32_t* b, uint32_t* c);

@@ -55,4 +55,16 @@ cudaError_t persistent_occupancy(size_t smem, int* ctas_per_sm);
 cudaError_t launch_persistent_rows(const BatchArgs& args, int logN2, int ctas, cudaStream_t s);
 cudaError_t persistent_rows_occupancy(int logN2, int* ctas_per_sm);
 
+// The 30-bit word engine (k_w32.cu): residues of operands [first, first + count), tiles
+// tile0 .. tile0 + tiles - 1 of each (128-coefficient tiles); the row stage; the CRT over
+// `tiles` 256-coefficient tiles.
+void* row32_kernel(const RowConfig& c);
+std::vector<RowConfig> all_row32_variants();
+size_t dec_tc32_smem_bytes(int k);
+cudaError_t prepare_w32();
+cudaError_t launch_residues32(const ProductDesc& d, const Tables& t, int logN1, cudaStream_t s, int first, int count,
+                              int tile0, int tiles);
+cudaError_t launch_row32(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s);
+cudaError_t launch_crt32(const ProductDesc& d, const Tables& t, int tiles, cudaStream_t s);
+
 }  // namespace nc

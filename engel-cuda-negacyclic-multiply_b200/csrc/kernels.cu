@@ -53,6 +53,7 @@ cudaError_t prepare_kernels(const PrimeConst* pc, const uint64_t* pow32) {
     if (e == cudaSuccess) e = prepare_crt_tc(pc, pow32);
     if (e == cudaSuccess) e = prepare_persistent(pc, pow32);
     if (e == cudaSuccess) e = prepare_residues(pc, pow32);
+    if (e == cudaSuccess) e = prepare_w32();
     return e;
 }
 
@@ -73,6 +74,7 @@ cudaError_t launch_residues(const ProductDesc& d, const Tables& t, const RowConf
     if (groups < 1 || group < 0 || group >= groups || all % groups != 0) return cudaErrorInvalidValue;
     int tiles = all / groups;
     int tile0 = group * tiles;
+    if (d.qc32) return launch_residues32(d, t, int(d.logN) - cfg.logN2, s, first, count, tile0, tiles);
     void* args[] = {&dd, &tt, &first, &tile0, &tiles};
     if (d.res_tc) {
         // tensor-core residues: 128-coefficient tiles
@@ -88,9 +90,11 @@ cudaError_t launch_residues(const ProductDesc& d, const Tables& t, const RowConf
 cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s,
                            cudaEvent_t* ev, cudaEvent_t b_ready, bool residues_done) {
     if (int(d.logN2) != cfg.logN2) return cudaErrorInvalidValue;
-    void* row = row_kernel(cfg);
+    const bool w32 = d.qc32 != nullptr;
+    void* row = w32 ? row32_kernel(cfg) : row_kernel(cfg);
     void* crt = d.crt_b ? crt_tc_kernel(int(d.LW)) : crt_kernel(int(d.LW));
     if (!row || !crt || !dec_kernel(int(d.LW))) return cudaErrorInvalidValue;
+    if (w32 && d.factors != 2) return cudaErrorInvalidValue;  // the 30-bit engine multiplies pairs
     const Geometry g = geometry(int(d.logN), int(d.k), cfg);
     ProductDesc dd = d;
     Tables tt = t;
@@ -110,16 +114,22 @@ cudaError_t launch_product(const ProductDesc& d, const Tables& t, const RowConfi
         if ((e = launch_residues(d, t, cfg, s, first, factors)) != cudaSuccess) return e;
     }
     if (ev && (e = cudaEventRecord(ev[1], s)) != cudaSuccess) return e;
-    {
+    if (w32) {
+        e = launch_row32(d, t, cfg, s);
+    } else {
         void* args[] = {&dd, &tt};
         e = launch(row, g.row_ctas, cfg.threads, row_smem_bytes(cfg.threads, cfg.logE), s, args);
-        if (e != cudaSuccess) return e;
     }
+    if (e != cudaSuccess) return e;
     if (ev && (e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
     if (d.mode != kModeForward) {
-        void* args[] = {&dd, &tt};
-        e = launch(crt, g.tiles, kThreads, d.crt_b ? crt_tc_smem_bytes(int(d.LW)) : crt_smem_bytes(int(d.k)), s,
-                   args);
+        if (w32) {
+            e = launch_crt32(d, t, g.tiles, s);
+        } else {
+            void* args[] = {&dd, &tt};
+            e = launch(crt, g.tiles, kThreads, d.crt_b ? crt_tc_smem_bytes(int(d.LW)) : crt_smem_bytes(int(d.k)), s,
+                       args);
+        }
         if (e != cudaSuccess) return e;
     }
     if (ev && (e = cudaEventRecord(ev[3], s)) != cudaSuccess) return e;

@@ -1,0 +1,284 @@
+// The 30-bit word engine: residues modulo primes p < 2^30 with p = 1 (mod 2^17), one 32-bit word
+// each, for the plain product of two operands.
+//
+// A 62-bit residue costs a 64 x 64-bit Shoup product per butterfly (about 17 integer multiply-adds
+// and as many ALU operations on the GPU's 32-bit datapath); a 30-bit residue costs one
+// multiply-high and two multiply-lows. Twice as many primes cover the same bound, so a product
+// does twice the butterflies at about a third of the instructions each. The stages and their
+// order are those of the 62-bit engine (stages.cuh): residues + forward column stages, row
+// blocks (forward a, forward b, pointwise, inverse), inverse column stages + CRT. Values stay
+// lazily reduced: forward (Cooley-Tukey) butterflies in [0, 4p), inverse (Gentleman-Sande) in
+// [0, 2p), which 4p < 2^32 allows. The pointwise product is a Montgomery product (its 2^-32 is
+// folded into the CRT constant of each prime).
+#pragma once
+
+#include <cstdint>
+
+#include "stages.cuh"
+
+namespace nc {
+
+namespace w32 {
+
+// x - m if x >= m, else x, for x < 2m <= 2^31 (x - m wraps above x when x < m).
+__device__ __forceinline__ uint32_t csub(uint32_t x, uint32_t m) { return min(x, x - m); }
+
+// y w mod p in [0, 2p) for any y < 2^32 and w < p, with wq = floor(w 2^32 / p).
+__device__ __forceinline__ uint32_t shoup(uint32_t y, uint32_t w, uint32_t wq, uint32_t p) {
+    return y * w - __umulhi(y, wq) * p;
+}
+
+// Forward butterfly (x, y) -> (x + w y, x - w y); inputs and outputs in [0, 4p).
+__device__ __forceinline__ void ct_bfly(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p, uint32_t p2) {
+    const uint32_t u = csub(x, p2);
+    const uint32_t t = shoup(y, w, wq, p);
+    x = u + t;
+    y = u - t + p2;
+}
+
+// Inverse butterfly (x, y) -> (x + y, (x - y) w); inputs and outputs in [0, 2p).
+__device__ __forceinline__ void gs_bfly(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p, uint32_t p2) {
+    const uint32_t s = csub(x + y, p2);
+    const uint32_t d = x - y + p2;
+    x = s;
+    y = shoup(d, w, wq, p);
+}
+
+// a b 2^-32 mod p in [0, 2p) for a < p, b < 4p (Montgomery; pinv = -p^-1 mod 2^32): the sum
+// a b + m p stays below 2^63 and its high word below p (4 p^2 / 2^32) + p.
+__device__ __forceinline__ uint32_t mont(uint32_t a, uint32_t b, uint32_t p, uint32_t pinv) {
+    const uint64_t t = uint64_t(a) * b;
+    const uint32_t m = uint32_t(t) * pinv;
+    return uint32_t((t + uint64_t(m) * p) >> 32);
+}
+
+// 16-byte-chunk XOR swizzle inside 128-byte rows of a u32 buffer (four words a chunk).
+__device__ __forceinline__ int swz(int x) {
+    const int c = x >> 2;
+    const int pc = (c & ~7) | ((c ^ (c >> 3)) & 7);
+    return (pc << 2) | (x & 3);
+}
+
+// ------------------------------------------------------------------------------------------
+// column stages (registers), as column_forward / column_inverse of the 62-bit engine
+
+template <int LOG_N1>
+__device__ __forceinline__ void column_forward_root(const uint2* tw, int root, uint32_t p, uint32_t (&v)[1 << LOG_N1]) {
+    constexpr int N1 = 1 << LOG_N1;
+    const uint32_t p2 = 2 * p;
+#pragma unroll
+    for (int s = 0; s < LOG_N1; ++s) {
+        const int half = N1 >> (s + 1);
+#pragma unroll
+        for (int blk = 0; blk < (1 << s); ++blk) {
+            const uint2 w = __ldg(tw + (root << s) + blk);
+#pragma unroll
+            for (int jj = 0; jj < half; ++jj) {
+                const int u = blk * 2 * half + jj;
+                ct_bfly(v[u], v[u + half], w.x, w.y, p, p2);
+            }
+        }
+    }
+}
+
+template <int LOG_N1>
+__device__ __forceinline__ void column_inverse_root(const uint2* tw, int root, uint32_t p, uint32_t (&v)[1 << LOG_N1]) {
+    constexpr int N1 = 1 << LOG_N1;
+    const uint32_t p2 = 2 * p;
+#pragma unroll
+    for (int s = LOG_N1 - 1; s >= 0; --s) {
+        const int half = N1 >> (s + 1);
+#pragma unroll
+        for (int blk = 0; blk < (1 << s); ++blk) {
+            const uint2 w = __ldg(tw + (root << s) + blk);
+#pragma unroll
+            for (int jj = 0; jj < half; ++jj) {
+                const int u = blk * 2 * half + jj;
+                gs_bfly(v[u], v[u + half], w.x, w.y, p, p2);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// row blocks: the register passes of stages.cuh over u32 residues
+
+template <class S, int PASS, bool FWD>
+__device__ __forceinline__ void row_pass(uint32_t (&v)[S::E], const uint2* tw, int base, int lt, uint32_t p) {
+    constexpr int R = S::r(PASS), LL = S::lolog(PASS), L0 = S::l0(PASS);
+    const uint32_t p2 = 2 * p;
+#pragma unroll
+    for (int q = 0; q < (S::E >> R); ++q) {
+        const int g = lt + S::T * q;
+        const int hi = g >> LL;
+#pragma unroll
+        for (int jj = 0; jj < R; ++jj) {
+            const int j = FWD ? jj : R - 1 - jj;
+            const int half = 1 << (R - 1 - j);
+            const int twbase = (base << (L0 + j)) + (hi << j);
+#pragma unroll
+            for (int blk = 0; blk < (1 << j); ++blk) {
+                const uint2 w = __ldg(tw + twbase + blk);
+#pragma unroll
+                for (int s0 = 0; s0 < half; ++s0) {
+                    const int e = q * (1 << R) + blk * 2 * half + s0;
+                    if (FWD)
+                        ct_bfly(v[e], v[e + half], w.x, w.y, p, p2);
+                    else
+                        gs_bfly(v[e], v[e + half], w.x, w.y, p, p2);
+                }
+            }
+        }
+    }
+}
+
+// A thread's values of pass PASS to / from the row buffer. When the pass's groups are runs of
+// consecutive elements (lolog 0), each run of four (or two) goes as one 16-byte (8-byte) access.
+template <class S, int PASS>
+__device__ __forceinline__ void row_store(const uint32_t (&v)[S::E], uint32_t* buf, int lt) {
+    if constexpr (S::lolog(PASS) == 0 && S::r(PASS) >= 2) {
+#pragma unroll
+        for (int e = 0; e < S::E; e += 4) {
+            const int x = row_index<S, PASS>(lt, e);
+            reinterpret_cast<uint4*>(buf)[swz(x) >> 2] = make_uint4(v[e], v[e + 1], v[e + 2], v[e + 3]);
+        }
+    } else if constexpr (S::lolog(PASS) == 0 && S::r(PASS) == 1) {
+#pragma unroll
+        for (int e = 0; e < S::E; e += 2) {
+            const int x = row_index<S, PASS>(lt, e);
+            reinterpret_cast<uint2*>(buf)[swz(x) >> 1] = make_uint2(v[e], v[e + 1]);
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) buf[swz(row_index<S, PASS>(lt, e))] = v[e];
+    }
+}
+
+template <class S, int PASS>
+__device__ __forceinline__ void row_load(uint32_t (&v)[S::E], const uint32_t* buf, int lt) {
+    if constexpr (S::lolog(PASS) == 0 && S::r(PASS) >= 2) {
+#pragma unroll
+        for (int e = 0; e < S::E; e += 4) {
+            const uint4 q = reinterpret_cast<const uint4*>(buf)[swz(row_index<S, PASS>(lt, e)) >> 2];
+            v[e] = q.x;
+            v[e + 1] = q.y;
+            v[e + 2] = q.z;
+            v[e + 3] = q.w;
+        }
+    } else if constexpr (S::lolog(PASS) == 0 && S::r(PASS) == 1) {
+#pragma unroll
+        for (int e = 0; e < S::E; e += 2) {
+            const uint2 q = reinterpret_cast<const uint2*>(buf)[swz(row_index<S, PASS>(lt, e)) >> 1];
+            v[e] = q.x;
+            v[e + 1] = q.y;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) v[e] = buf[swz(row_index<S, PASS>(lt, e))];
+    }
+}
+
+template <class S, int PASS>
+__device__ __forceinline__ void row_forward_from(uint32_t (&v)[S::E], uint32_t* buf, const uint2* tw, int base, int lt,
+                                                 uint32_t p) {
+    row_pass<S, PASS, true>(v, tw, base, lt, p);
+    if constexpr (PASS + 1 < S::NPASS) {
+        __syncthreads();
+        row_store<S, PASS>(v, buf, lt);
+        __syncthreads();
+        row_load<S, PASS + 1>(v, buf, lt);
+        row_forward_from<S, PASS + 1>(v, buf, tw, base, lt, p);
+    }
+}
+
+template <class S, int PASS>
+__device__ __forceinline__ void row_inverse_from(uint32_t (&v)[S::E], uint32_t* buf, const uint2* tw, int base, int lt,
+                                                 uint32_t p) {
+    row_pass<S, PASS, false>(v, tw, base, lt, p);
+    if constexpr (PASS > 0) {
+        __syncthreads();
+        row_store<S, PASS>(v, buf, lt);
+        __syncthreads();
+        row_load<S, PASS - 1>(v, buf, lt);
+        row_inverse_from<S, PASS - 1>(v, buf, tw, base, lt, p);
+    }
+}
+
+// Dynamic shared memory of a row CTA: the row buffer and the buffer of operand a's transform.
+NC_HD constexpr size_t row_smem_bytes(int threads, int logE) { return size_t(2) * size_t(threads) * (size_t(1) << logE) * 4; }
+
+// One CTA of THREADS threads handles THREADS / T row blocks, as row_blocks of stages.cuh: block
+// rb = item * ROWS + (tid / T) is prime rb >> logN1, row u = rb & (N1 - 1). Modes: product
+// (forward a and b, pointwise, inverse), cached-a (a's transform read from a_hat), forward (a's
+// transform written to hat_out). Residues are k x N u32.
+template <int LOG_N2, int LOG_E, int THREADS>
+__device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint8_t* smem) {
+    using S = RowShape<LOG_N2, LOG_E>;
+    static_assert(S::T <= THREADS, "row block needs more threads than the CTA has");
+    constexpr int ROWS = THREADS / S::T;
+    constexpr int LAST = S::NPASS - 1;
+    const int logN1 = int(d.logN) - LOG_N2;
+    const int N = 1 << d.logN;
+    const int rr = threadIdx.x / S::T, lt = threadIdx.x - rr * S::T;
+    const int rb = item * ROWS + rr;
+    const bool active = rb < (int(d.k) << logN1);
+    const int i = active ? rb >> logN1 : 0;
+    const int u = rb & ((1 << logN1) - 1);
+    const uint32_t p = __ldg(&t.pc32[i].p), pinv = __ldg(&t.pc32[i].pinv);
+    const int base = (1 << logN1) + u;
+    const size_t off = size_t(i) * N + size_t(u) * S::N2;
+    uint32_t* buf = reinterpret_cast<uint32_t*>(smem) + rr * S::N2;
+    uint32_t* buf_a = reinterpret_cast<uint32_t*>(smem) + size_t(ROWS) * S::N2 + rr * S::N2;
+    const uint2* twf = t.fwd32 + size_t(i) * kMaxN;
+    const uint2* twi = t.inv32 + size_t(i) * kMaxN;
+    const uint32_t* ra = reinterpret_cast<const uint32_t*>(d.ra);
+    const uint32_t* rb_res = reinterpret_cast<const uint32_t*>(d.rb);
+    uint32_t v[S::E];
+
+    __syncthreads();  // shared memory of a previous item is free
+    pdl_wait();       // the residues come from the stream's previous kernel
+    if (d.mode == kModeCachedA) {
+        const uint32_t* a_hat = reinterpret_cast<const uint32_t*>(d.a_hat);
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) {
+            const int x = row_index<S, 0>(lt, e);
+            buf_a[swz(x)] = active ? __ldcg(a_hat + off + x) : 0u;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(ra + off + row_index<S, 0>(lt, e)) : 0u;
+        row_forward_from<S, 0>(v, buf, twf, base, lt, p);
+        if (d.mode == kModeForward) {
+            __syncthreads();
+            row_store<S, LAST>(v, buf, lt);
+            __syncthreads();
+            row_load<S, 0>(v, buf, lt);
+            if (active) {
+                uint32_t* out = reinterpret_cast<uint32_t*>(d.hat_out);
+#pragma unroll
+                for (int e = 0; e < S::E; ++e) __stcg(out + off + row_index<S, 0>(lt, e), v[e]);
+            }
+            return;
+        }
+        row_store<S, LAST>(v, buf_a, lt);
+    }
+#pragma unroll
+    for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(rb_res + off + row_index<S, 0>(lt, e)) : 0u;
+    row_forward_from<S, 0>(v, buf, twf, base, lt, p);
+    __syncthreads();
+    const uint32_t p2 = 2 * p;
+    uint32_t av[S::E];
+    row_load<S, LAST>(av, buf_a, lt);
+#pragma unroll
+    for (int e = 0; e < S::E; ++e) v[e] = mont(csub(csub(av[e], p2), p), v[e], p, pinv);
+    row_inverse_from<S, LAST>(v, buf, twi, base, lt, p);
+    if (active) {
+        uint32_t* out = reinterpret_cast<uint32_t*>(d.ra);
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) __stcg(out + off + row_index<S, 0>(lt, e), v[e]);
+    }
+}
+
+}  // namespace w32
+
+}  // namespace nc

@@ -58,6 +58,9 @@ C_SYMBOLS = [
     ("nc_plan_get_row_config", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int)]),
     ("nc_plan_autotune", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    ("nc_row_variants32", ctypes.c_int, [ctypes.c_uint32, ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    ("nc_plan_set_word_bits", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("nc_plan_word_bits", ctypes.c_int, [_vp, _u32p]),
     ("nc_batch_create", ctypes.c_int, [ctypes.POINTER(_vp)]),
     ("nc_batch_destroy", ctypes.c_int, [_vp]),
     ("nc_batch_add", ctypes.c_int, [_vp, _vp, _vp, _vp, _vp]),
@@ -154,9 +157,10 @@ def residues_gave_up() -> bool:
 class Plan:
     """One (N, q) configuration on the current CUDA device."""
 
-    def __init__(self, N: int, q_limbs: np.ndarray, W: int = 0, factors: int = 2):
+    def __init__(self, N: int, q_limbs: np.ndarray, W: int = 0, factors: int = 2, word_bits: int | None = None):
         """factors > 2 makes a chain plan: its primes cover products of that many operands
-        (multiply_chain); it still runs ordinary two-operand products."""
+        (multiply_chain); it still runs ordinary two-operand products. word_bits (32 or 64) picks
+        the plain path's residue engine (default: the library's choice; see word_bits)."""
         q = np.ascontiguousarray(q_limbs, dtype=np.uint32)
         self.N, self.L = int(N), int(q.size)
         self._h = _vp()
@@ -168,6 +172,31 @@ class Plan:
         n, l, k, qb = (ctypes.c_uint32() for _ in range(4))
         _check(load().nc_plan_query(self._h, ctypes.byref(n), ctypes.byref(l), ctypes.byref(k), ctypes.byref(qb)))
         self.k, self.qbits = int(k.value), int(qb.value)
+        if word_bits is not None:
+            self.word_bits = word_bits
+
+    @property
+    def word_bits(self) -> int:
+        """32 (the 30-bit engine: u32 residues modulo primes below 2^30) or 64 (the 62-bit engine)
+        for this plan's plain-path products; the engine in use."""
+        v = load().nc_plan_word_bits(self._h, None)
+        if v < 0:
+            _check(v)
+        return v
+
+    @word_bits.setter
+    def word_bits(self, bits: int) -> None:
+        _check(load().nc_plan_set_word_bits(self._h, int(bits)))
+
+    @property
+    def plain_primes(self) -> int:
+        """Residue primes of the plain path's engine in use (k of the 62-bit engine, or the
+        30-bit engine's count)."""
+        k = ctypes.c_uint32()
+        v = load().nc_plan_word_bits(self._h, ctypes.byref(k))
+        if v < 0:
+            _check(v)
+        return int(k.value)
 
     @property
     def handle(self) -> int:
@@ -295,13 +324,15 @@ class Plan:
             pass
 
 
-def row_variants(log_n: int) -> list[tuple[int, int, int]]:
-    """Compiled row configurations (log_block, log_radix, threads) valid for N = 2^log_n."""
-    n = load().nc_row_variants(int(log_n), None, 0)
+def row_variants(log_n: int, word_bits: int = 64) -> list[tuple[int, int, int]]:
+    """Compiled row configurations (log_block, log_radix, threads) valid for N = 2^log_n, of the
+    62-bit engine (word_bits 64) or the 30-bit engine (32)."""
+    fn = load().nc_row_variants if word_bits == 64 else load().nc_row_variants32
+    n = fn(int(log_n), None, 0)
     if n < 0:
         _check(n)
     buf = (ctypes.c_int * (3 * max(n, 1)))()
-    got = load().nc_row_variants(int(log_n), buf, n)
+    got = fn(int(log_n), buf, n)
     return [(buf[3 * i], buf[3 * i + 1], buf[3 * i + 2]) for i in range(got)]
 
 

@@ -177,6 +177,24 @@ int nc_row_variants(uint32_t log_n, int* triples, int max_variants);
 int nc_plan_set_row_config(nc_plan* plan, int log_block, int log_radix, int threads);
 int nc_plan_get_row_config(const nc_plan* plan, int* log_block, int* log_radix, int* threads);
 
+/* Word size of the plain path's residues. 64: the 62-bit engine (primes 2^62 - m; every plan).
+   32: the 30-bit engine, primes p < 2^30 with p = 1 (mod 2^17), one u32 residue each, about twice
+   as many primes at a third of the instructions per butterfly; it needs a compute capability 10.0
+   device (its residue and CRT stages run on the tensor cores), a product of two operands, and a
+   coefficient bound within 64 such primes (q up to 948 bits at N = 65536). It is the default
+   where it can run (NC_WORD_BITS=64 in the environment keeps the 62-bit engine), the autotuner
+   keeps the faster of the two, and it is in use only while both tensor-core stages are selected
+   (nc_plan_set_residue_engine / nc_plan_set_crt_engine to the integer pipes select the 62-bit
+   engine). Row configurations (nc_plan_set_row_config / get) apply to the engine in use;
+   nc_row_variants32 lists the 30-bit engine's as nc_row_variants lists the 62-bit one's. Batches,
+   servers, chained products and nc_multiply_device_noalloc run the 62-bit engine.
+   nc_plan_word_bits returns 32 or 64 (the engine in use) and writes its prime count to k (may be
+   NULL); nc_plan_set_word_bits fails with NC_EINVAL where the 30-bit engine cannot run. Both
+   engines give the same product. Set it only while no product of the plan is in flight. */
+int nc_row_variants32(uint32_t log_n, int* triples, int max_variants);
+int nc_plan_set_word_bits(nc_plan* plan, int bits);
+int nc_plan_word_bits(const nc_plan* plan, uint32_t* k);
+
 /* Autotuner: times every compiled row configuration for the plan's N on the device (`reps`
    products each), keeps the fastest for this plan and for later plans of the same (N, L) in
    this process, and writes its milliseconds per product to best_ms (may be NULL). */

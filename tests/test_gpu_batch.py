@@ -28,7 +28,7 @@ def test_every_row_variant(gpu, log_n):
     want = oracle.negacyclic(N, c.q_limbs, c.a, c.b)
     variants = nc.row_variants(log_n)
     assert variants
-    with nc.Plan(N, c.q_limbs) as plan:
+    with nc.Plan(N, c.q_limbs, word_bits=64) as plan:
         for cfg in variants:
             plan.row_config = cfg
             assert plan.row_config == cfg
@@ -41,11 +41,11 @@ def test_autotune_keeps_results_exact(gpu):
     with nc.Plan(c.N, c.q_limbs) as plan:
         ms = plan.autotune(reps=2)
         assert ms > 0
-        assert plan.row_config in nc.row_variants(14)
+        assert plan.row_config in nc.row_variants(14, word_bits=plan.word_bits)
         assert np.array_equal(plan.multiply(c.a, c.b), oracle.negacyclic(c.N, c.q_limbs, c.a, c.b))
         # later plans of the same (N, L) start from the tuned choice
         with nc.Plan(c.N, c.q_limbs) as p2:
-            assert p2.row_config == plan.row_config
+            assert p2.word_bits == plan.word_bits and p2.row_config == plan.row_config
 
 
 def _run_batch(gpu, specs, use_graph=True, repeat=1):

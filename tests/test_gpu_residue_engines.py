@@ -44,7 +44,7 @@ def test_every_column_length(gpu, N, cfg):
     assert cfg in nc.row_variants(N.bit_length() - 1)
     c = cases.make_case(N, 868, seed=N + cfg[0], edge_frac=0.02)
     want = oracle.negacyclic(N, c.q_limbs, c.a, c.b)
-    with nc.Plan(N, c.q_limbs) as plan:
+    with nc.Plan(N, c.q_limbs, word_bits=64) as plan:
         plan.row_config = cfg
         got = _both_engines(plan, c.a, c.b)
     assert np.array_equal(got[nc.RESIDUES_TC_I8], want)
