@@ -79,6 +79,9 @@ def parse_args():
                     help="each rep is one batch of this many products (persistent launch) instead of one product")
     pc.add_argument("--profile-residue-engine", choices=["tc", "imad"], default="tc",
                     help="residue stage of the products: k_dec_tc (tensor cores) or k_dec (integer pipes)")
+    pc.add_argument("--profile-word-bits", type=int, choices=[0, 32, 64], default=0,
+                    help="the plain path's engine (32: the 30-bit word engine, 64: the 62-bit engine; "
+                         "0: the library's default)")
     pc.add_argument("--profile-residues", choices=["", "imad", "tc"], default="",
                     help="run only the residue stage of both operands with this engine (k_residues_imad / "
                          "k_residues_tc), checked against the other engine")
@@ -162,12 +165,16 @@ class ClockSampler:
 # ----------------------------------------------------------------------------- roofline
 
 
-def stage_work(k: int, N: int, L: int, logN2: int | None = None) -> list[float]:
-    """Algorithmic IMAD per stage: 8 per 64-bit mulmod, 2 per u32 x u64 limb MAC, 4 L per
-    coefficient for the final reduction. Whole product: 8 k N (1.5 log2 N + 7) + 6 k N L + 4 L N.
-    logN2 is the row block of the plan's row configuration (its row kernel runs logN2 stages of
-    each transform; the residue and CRT kernels run the other logN1 = log2 N - logN2 column
-    stages); the per-stage split depends on it, the product total does not."""
+def stage_work(k: int, N: int, L: int, logN2: int | None = None, word_bits: int = 64) -> list[float]:
+    """Algorithmic IMAD per stage. 62-bit engine (word_bits 64): 8 per 64-bit mulmod (the four
+    32 x 32 partial products of a 64 x 64 product, low and high halves), 2 per u32 x u64 limb MAC;
+    whole product 8 k N (1.5 log2 N + 7) + 6 k N L + 4 L N. 30-bit engine (word_bits 32): 3 per
+    30-bit mulmod (a Shoup or Montgomery product: one high and two low 32 x 32 products), 1 per
+    u32 x u32 limb MAC; whole product 3 k N (1.5 log2 N + 7) + 3 k N L + 4 L N. Both count 4 L per
+    coefficient for the final reduction. logN2 is the row block of the plan's row configuration
+    (its row kernel runs logN2 stages of each transform; the residue and CRT kernels run the
+    other logN1 = log2 N - logN2 column stages); the per-stage split depends on it, the product
+    total does not."""
     logN = N.bit_length() - 1
     if logN2 is None:
         logN2 = min(logN, 12)
@@ -179,15 +186,17 @@ def stage_work(k: int, N: int, L: int, logN2: int | None = None) -> list[float]:
     mm2 = 3 * k * (N // 2) * logN2 + k * N                    # three row transforms, pointwise
     mm3 = k * (N // 2) * logN1 + k * N + k * N                # inverse column stages, untwist, CRT digit
     mac3 = k * N * L
-    return [8 * mm1 + 2 * mac1, 8 * mm2, 8 * mm3 + 2 * mac3 + 4 * L * N]
+    mm, mac = (8, 2) if word_bits == 64 else (3, 1)
+    return [mm * mm1 + mac * mac1, mm * mm2, mm * mm3 + mac * mac3 + 4 * L * N]
 
 
-def stage_bytes(k: int, N: int, L: int) -> list[int]:
-    """Compulsory HBM bytes per stage (operands, residues, twiddles read once)."""
-    logN = N.bit_length() - 1
-    return [2 * N * L * 4 + 2 * k * N * 8,
-            2 * k * N * 8 + k * N * 8 + 2 * k * N * 16,
-            k * N * 8 + N * L * 4]
+def stage_bytes(k: int, N: int, L: int, word_bits: int = 64) -> list[int]:
+    """Compulsory HBM bytes per stage (operands, residues, twiddles read once): residues of
+    word_bits / 8 bytes, twiddles with their Shoup companions twice that."""
+    r = word_bits // 8
+    return [2 * N * L * 4 + 2 * k * N * r,
+            2 * k * N * r + k * N * r + 2 * k * N * 2 * r,
+            k * N * r + N * L * 4]
 
 
 # ----------------------------------------------------------------------------- harness runs
@@ -379,17 +388,20 @@ def ours(args) -> dict | None:
     total_ms, batch_ms = max_over_ranks(pg, [total_ms, batch_ms], dev)
 
     peak = nc.imad_peak()
-    k, N, L = plan.k, case.N, case.L
+    word, k, N, L = plan.word_bits, plan.plain_primes, case.N, case.L
     mean_stage = [statistics.mean(s[i] for s in stage) for i in range(3)]
-    work = stage_work(k, N, L, plan.row_config[0])
-    sbytes = stage_bytes(k, N, L)
+    work = stage_work(k, N, L, plan.row_config[0], word)
+    sbytes = stage_bytes(k, N, L, word)
     dom = max(range(3), key=lambda i: mean_stage[i])
     crt_tc = plan.crt_engine == nc.CRT_TC_I8
     res_tc = plan.residue_engine == nc.RESIDUES_TC_I8
     names = ["residues (contraction on the tensor cores)+forward columns" if res_tc else "residues+forward columns",
              "row NTTs+pointwise",
              "inverse columns+CRT (accumulation on the tensor cores)" if crt_tc else "inverse columns+CRT"]
-    kernels = ["k_dec_tc" if res_tc else "k_dec", "k_row", "k_crt_tc" if crt_tc else "k_crt"]
+    if word == 32:
+        kernels = ["k_dec_tc32", "k_row32", "k_crt_tc32"]
+    else:
+        kernels = ["k_dec_tc" if res_tc else "k_dec", "k_row", "k_crt_tc" if crt_tc else "k_crt"]
     traffic = None
     if TRAFFIC_FILE.exists():
         tf = json.loads(TRAFFIC_FILE.read_text())
@@ -406,10 +418,13 @@ def ours(args) -> dict | None:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "u64",
+        "dtype": "u32" if word == 32 else "u64",
         "data": "synthetic (seeded)",
         "config": config(f"replicas{world}"),
         "gpu_launches": 3 * args.steps,
+        "engine": {"word_bits": word, "primes": k,
+                   "what": ("30-bit word engine: u32 residues modulo primes below 2^30" if word == 32 else
+                            "62-bit engine: u64 residues modulo primes 2^62 - m")},
         "row_config": {"log_block": plan.row_config[0], "log_radix": plan.row_config[1],
                        "threads": plan.row_config[2], "autotune_ms": tuned_ms},
         "roofline": {
@@ -992,6 +1007,8 @@ def profile_case(a) -> int:
     count = max(1, a.profile_batch)
     dcs = [torch.empty_like(da) for _ in range(count)]
     with nc.Plan(case.N, case.q_limbs, W=case.W) as plan:
+        if a.profile_word_bits:
+            plan.word_bits = a.profile_word_bits
         if a.row_config:
             plan.row_config = tuple(int(x) for x in a.row_config.split(","))
         if a.profile_residue_engine == "imad" or plan.k > 32:

@@ -96,9 +96,18 @@ void Batch::finalize(cudaStream_t stream) {
     std::vector<uint64_t> shape;
     size_t scratch = 0;
     int kmax = 1, kmax_imad = 0, kmax_tc = 0;
+    // products that fill the GPU alone run the plain path's launches, on the plan's 30-bit engine
+    // where it runs (plain products whose residue scratch comes from the batch's arena)
+    auto direct_w32 = [](const Entry& e) {
+        return e.plan->logN >= kDirectLogN && e.mode == kModeProduct && !e.scratch && e.plan->use_w32();
+    };
+    auto residue_bytes = [&](const Entry& e) {
+        return round_up(direct_w32(e) ? e.plan->residue_bytes() : size_t(e.plan->k) * e.plan->N * sizeof(uint64_t),
+                        256);
+    };
     for (size_t p = 0; p < n; ++p) {
         const Plan* pl = entries_[p].plan;
-        if (!entries_[p].scratch) scratch += 2 * round_up(size_t(pl->k) * pl->N * sizeof(uint64_t), 256);
+        if (!entries_[p].scratch) scratch += 2 * residue_bytes(entries_[p]);
         kmax = std::max(kmax, pl->k);
         (pl->res_tc ? kmax_tc : kmax_imad) = std::max(pl->res_tc ? kmax_tc : kmax_imad, pl->k);
     }
@@ -125,7 +134,7 @@ void Batch::finalize(cudaStream_t stream) {
         d.mode = e.mode;
         d.a_hat = e.a_hat;
         d.hat_out = e.hat_out;
-        const size_t res = round_up(size_t(pl->k) * pl->N * sizeof(uint64_t), 256);
+        const size_t res = residue_bytes(e);
         if (e.scratch) {
             d.ra = e.scratch;
             d.rb = e.scratch + res / sizeof(uint64_t);
@@ -136,11 +145,19 @@ void Batch::finalize(cudaStream_t stream) {
         }
         if (pl->logN >= kDirectLogN) {
             // fills the GPU alone: the plain path's launches with the plan's row configuration
-            d.logN2 = uint32_t(pl->cfg.logN2);
-            direct_.push_back(Direct{d, pl->cfg});
-            shape.push_back((uint64_t(1) << 63) | (uint64_t(pl->logN) << 40) | (uint64_t(pl->k) << 32) |
-                            (uint64_t(pl->cfg.logN2) << 24) | (uint64_t(pl->cfg.logE) << 16) |
-                            (uint64_t(pl->cfg.threads) << 4) | e.mode);
+            const bool w32 = direct_w32(e);
+            const RowConfig& dc = w32 ? pl->cfg32 : pl->cfg;
+            if (w32) {
+                ProductDesc dw = pl->desc_plain(e.a, e.b, e.c);
+                dw.ra = d.ra;
+                dw.rb = d.rb;
+                d = dw;
+            }
+            d.logN2 = uint32_t(dc.logN2);
+            direct_.push_back(Direct{d, dc});
+            shape.push_back((uint64_t(1) << 63) | (uint64_t(w32) << 62) | (uint64_t(pl->logN) << 40) |
+                            (uint64_t(d.k) << 32) | (uint64_t(dc.logN2) << 24) | (uint64_t(dc.logE) << 16) |
+                            (uint64_t(dc.threads) << 4) | e.mode);
             continue;
         }
         BatchProduct& bp = prods[p];

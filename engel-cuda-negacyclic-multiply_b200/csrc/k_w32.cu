@@ -544,8 +544,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_crt_tc32(ProductDesc d, Tables 
 template <int LOG_N2, int LOG_E, int THREADS>
 __global__ void __launch_bounds__(THREADS, (THREADS == 256 ? (LOG_E == 3 ? 4 : 3) : 2)) k_row32(ProductDesc d, Tables t) {
     extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint64_t tw_bar;
     pdl_trigger();
-    w32::row_blocks<LOG_N2, LOG_E, THREADS>(d, t, int(blockIdx.x), smem);
+    w32::row_blocks<LOG_N2, LOG_E, THREADS>(d, t, int(blockIdx.x), smem, &tw_bar);
 }
 
 #define NC_ROW32_VARIANTS(X)                                                                                   \

@@ -118,7 +118,7 @@ __device__ __forceinline__ void row_pass(uint32_t (&v)[S::E], const uint2* tw, i
             const int twbase = (base << (L0 + j)) + (hi << j);
 #pragma unroll
             for (int blk = 0; blk < (1 << j); ++blk) {
-                const uint2 w = __ldg(tw + twbase + blk);
+                const uint2 w = tw[twbase + blk];  // shared memory (stage_twiddles)
 #pragma unroll
                 for (int s0 = 0; s0 < half; ++s0) {
                     const int e = q * (1 << R) + blk * 2 * half + s0;
@@ -204,15 +204,66 @@ __device__ __forceinline__ void row_inverse_from(uint32_t (&v)[S::E], uint32_t* 
     }
 }
 
-// Dynamic shared memory of a row CTA: the row buffer and the buffer of operand a's transform.
-NC_HD constexpr size_t row_smem_bytes(int threads, int logE) { return size_t(2) * size_t(threads) * (size_t(1) << logE) * 4; }
+// Dynamic shared memory of a row CTA: the row buffer and the buffer of operand a's transform
+// (4 bytes a residue each), then each row block's forward and inverse twiddles (8 bytes an entry,
+// N2 entries each).
+NC_HD constexpr size_t row_smem_bytes(int threads, int logE) { return size_t(threads) * (size_t(1) << logE) * 24; }
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Bounded wait for phase `parity` of the mbarrier at shared address `bar`: false if it did not
+// complete within 2^22 polls.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// The twiddles of the row block under node `base` of the merged tree: local stage l uses the 2^l
+// entries tw[(base << l) + t], stored at s[(1 << l) + t] (entry 0 unused), so that the row passes
+// read them from shared memory with base 1. Stages l >= 1 go as bulk copies (2^l entries of 8
+// bytes: 16-byte aligned and a multiple of 16 bytes at both ends) that complete on the mbarrier
+// `bar`; stage 0's single entry as a plain load.
+template <int LOG_N2>
+__device__ __forceinline__ void stage_twiddles(const uint2* tw, int base, uint2* s, uint32_t bar) {
+    s[1] = __ldg(tw + base);
+#pragma unroll
+    for (int l = 1; l < LOG_N2; ++l)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(s + (1 << l))),
+                     "l"(tw + (size_t(base) << l)), "r"(8u << l), "r"(bar)
+                     : "memory");
+}
+
+// The same entries by plain loads, every thread of the CTA taking its share (the fallback if the
+// bulk copies do not complete in time).
+template <int LOG_N2>
+__device__ __forceinline__ void copy_twiddles(const uint2* tw, int base, uint2* s, int part, int parts) {
+    for (int e = 1 + part; e < (1 << LOG_N2); e += parts) {
+        const int l = 31 - __clz(e);
+        s[e] = __ldg(tw + (size_t(base) << l) + (e - (1 << l)));
+    }
+}
 
 // One CTA of THREADS threads handles THREADS / T row blocks, as row_blocks of stages.cuh: block
 // rb = item * ROWS + (tid / T) is prime rb >> logN1, row u = rb & (N1 - 1). Modes: product
 // (forward a and b, pointwise, inverse), cached-a (a's transform read from a_hat), forward (a's
-// transform written to hat_out). Residues are k x N u32.
+// transform written to hat_out). Residues are k x N u32. The twiddles of each row block are staged
+// in shared memory at the start (bulk copies on the CTA's mbarrier `tw_bar`, overlapping the
+// residue loads): the passes then wait on no global load but the residues. One launch per CTA
+// (the mbarrier's phase 0).
 template <int LOG_N2, int LOG_E, int THREADS>
-__device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint8_t* smem) {
+__device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint8_t* smem,
+                                           uint64_t* tw_bar) {
     using S = RowShape<LOG_N2, LOG_E>;
     static_assert(S::T <= THREADS, "row block needs more threads than the CTA has");
     constexpr int ROWS = THREADS / S::T;
@@ -229,14 +280,44 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
     const size_t off = size_t(i) * N + size_t(u) * S::N2;
     uint32_t* buf = reinterpret_cast<uint32_t*>(smem) + rr * S::N2;
     uint32_t* buf_a = reinterpret_cast<uint32_t*>(smem) + size_t(ROWS) * S::N2 + rr * S::N2;
+    uint2* s_twf = reinterpret_cast<uint2*>(smem + size_t(2) * ROWS * S::N2 * 4) + size_t(rr) * 2 * S::N2;
+    uint2* s_twi = s_twf + S::N2;
     const uint2* twf = t.fwd32 + size_t(i) * kMaxN;
     const uint2* twi = t.inv32 + size_t(i) * kMaxN;
     const uint32_t* ra = reinterpret_cast<const uint32_t*>(d.ra);
     const uint32_t* rb_res = reinterpret_cast<const uint32_t*>(d.rb);
+    const uint32_t bar = smem_addr(tw_bar);
+    const bool inverse = d.mode != kModeForward;
     uint32_t v[S::E];
 
-    __syncthreads();  // shared memory of a previous item is free
-    pdl_wait();       // the residues come from the stream's previous kernel
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(ROWS) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (lt == 0) {
+        // the twiddle tables do not depend on the previous kernel: their copies start before its end
+        const uint32_t bytes = (inverse ? 2u : 1u) * 8u * ((1u << LOG_N2) - 2u);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        stage_twiddles<LOG_N2>(twf, base, s_twf, bar);
+        if (inverse) stage_twiddles<LOG_N2>(twi, base, s_twi, bar);
+    }
+    // every thread waits for the copies (bounded); if any gave up, each row's threads copy its
+    // twiddles themselves and, before the CTA exits, wait once more for the copies in flight
+    bool staged = true;
+    auto twiddles_ready = [&] {
+        staged = __syncthreads_and(bar_wait(bar, 0) ? 1 : 0) != 0;
+        if (!staged) {
+            copy_twiddles<LOG_N2>(twf, base, s_twf, lt, S::T);
+            if (inverse) copy_twiddles<LOG_N2>(twi, base, s_twi, lt, S::T);
+            __syncthreads();
+        }
+    };
+    auto finish = [&] {
+        if (!staged) bar_wait(bar, 0);
+    };
+
+    pdl_wait();  // the residues come from the stream's previous kernel
     if (d.mode == kModeCachedA) {
         const uint32_t* a_hat = reinterpret_cast<const uint32_t*>(d.a_hat);
 #pragma unroll
@@ -244,10 +325,14 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
             const int x = row_index<S, 0>(lt, e);
             buf_a[swz(x)] = active ? __ldcg(a_hat + off + x) : 0u;
         }
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(rb_res + off + row_index<S, 0>(lt, e)) : 0u;
+        twiddles_ready();
     } else {
 #pragma unroll
         for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(ra + off + row_index<S, 0>(lt, e)) : 0u;
-        row_forward_from<S, 0>(v, buf, twf, base, lt, p);
+        twiddles_ready();
+        row_forward_from<S, 0>(v, buf, s_twf, 1, lt, p);
         if (d.mode == kModeForward) {
             __syncthreads();
             row_store<S, LAST>(v, buf, lt);
@@ -258,25 +343,27 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
 #pragma unroll
                 for (int e = 0; e < S::E; ++e) __stcg(out + off + row_index<S, 0>(lt, e), v[e]);
             }
+            finish();
             return;
         }
         row_store<S, LAST>(v, buf_a, lt);
-    }
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(rb_res + off + row_index<S, 0>(lt, e)) : 0u;
-    row_forward_from<S, 0>(v, buf, twf, base, lt, p);
+        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(rb_res + off + row_index<S, 0>(lt, e)) : 0u;
+    }
+    row_forward_from<S, 0>(v, buf, s_twf, 1, lt, p);
     __syncthreads();
     const uint32_t p2 = 2 * p;
     uint32_t av[S::E];
     row_load<S, LAST>(av, buf_a, lt);
 #pragma unroll
     for (int e = 0; e < S::E; ++e) v[e] = mont(csub(csub(av[e], p2), p), v[e], p, pinv);
-    row_inverse_from<S, LAST>(v, buf, twi, base, lt, p);
+    row_inverse_from<S, LAST>(v, buf, s_twi, 1, lt, p);
     if (active) {
         uint32_t* out = reinterpret_cast<uint32_t*>(d.ra);
 #pragma unroll
         for (int e = 0; e < S::E; ++e) __stcg(out + off + row_index<S, 0>(lt, e), v[e]);
     }
+    finish();
 }
 
 }  // namespace w32
