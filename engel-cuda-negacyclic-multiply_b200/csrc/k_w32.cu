@@ -68,15 +68,17 @@ __device__ __forceinline__ int res_slot(int i, int x, int C) {
 // multiple of 16 columns), within the table's 64 primes.
 __host__ __device__ constexpr int dec32_weight_pairs(int k) { return ((k + 3) & ~3) / 2; }
 
-template <int LOG_N1>
+// CC: the tile's columns when N >= 128 (128 >> LOG_N1, a constant: the index arithmetic of the
+// fold and the column stages folds away), 0 for smaller N.
+template <int LOG_N1, int CC>
 __device__ __forceinline__ void dec_tc32_item(const ProductDesc& d, const Tables& t, int operand, int tile,
                                               uint8_t* smem, uint64_t& bar, uint32_t& taddr_slot) {
     constexpr int N1 = 1 << LOG_N1;
     const int N = 1 << d.logN;
     const int N2 = N >> LOG_N1;
-    const int T = N < kDecTcRows ? N : kDecTcRows;
-    const int logC = (N < kDecTcRows ? int(d.logN) : 7) - LOG_N1;
-    const int C = 1 << logC;
+    const int T = CC ? kDecTcRows : (N < kDecTcRows ? N : kDecTcRows);
+    const int logC = CC ? 7 - LOG_N1 : (N < kDecTcRows ? int(d.logN) : 7) - LOG_N1;
+    const int C = CC ? CC : 1 << logC;
     const int j0 = tile * C;
     const int L = int(d.L), k = int(d.k);
     const int wpairs = dec32_weight_pairs(k);
@@ -102,7 +104,7 @@ __device__ __forceinline__ void dec_tc32_item(const ProductDesc& d, const Tables
     pdl_trigger();
 
     for (int q = tid; q < wpairs * 64; q += kThreads) cp_async16(sB + q * 16, t.res_w32 + q);
-    for (int w = tid; w < k; w += kThreads) s_pc[w] = t.pc32[w];
+    for (int w = tid; w < ((k + 3) & ~3); w += kThreads) s_pc[w] = t.pc32[w];  // the MMAs' primes
     pdl_wait();  // the operand and the residue rows belong to the stream's previous kernels
     const int kbytes = 4 * L;
     for (int q = tid; q < kDecTcRows * 8; q += kThreads) {
@@ -176,10 +178,10 @@ __device__ __forceinline__ void dec_tc32_item(const ProductDesc& d, const Tables
                       "=r"(s[15])
                     : "r"(lane_base + uint32_t(4 * (i - i0))));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                // all four (primes up to k rounded up to four have weights, constants and rows)
 #pragma unroll
                 for (int e = 0; e < 4; ++e)
-                    if (i + e < ie)
-                        res_row(sB, i + e)[res_slot(i + e, m, C)] = fold_planes(s + 4 * e, s_pc[i + e].p, s_pc[i + e].bar);
+                    res_row(sB, i + e)[res_slot(i + e, m, C)] = fold_planes(s + 4 * e, s_pc[i + e].p, s_pc[i + e].bar);
             }
         } else if (m < T) {
             // the wait gave up: this warp's residues on the integer pipes
@@ -260,8 +262,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_dec_tc32(ProductDesc d, Tables 
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ uint64_t bar;
     __shared__ uint32_t taddr_slot;
-    dec_tc32_item<LOG_N1>(d, t, first_operand + int(blockIdx.x) / tiles, tile0 + int(blockIdx.x) % tiles, smem, bar,
-                          taddr_slot);
+    const int operand = first_operand + int(blockIdx.x) / tiles, tile = tile0 + int(blockIdx.x) % tiles;
+    if (d.logN >= 7)
+        dec_tc32_item<LOG_N1, (kDecTcRows >> LOG_N1)>(d, t, operand, tile, smem, bar, taddr_slot);
+    else
+        dec_tc32_item<LOG_N1, 0>(d, t, operand, tile, smem, bar, taddr_slot);
 #endif
 }
 
