@@ -204,10 +204,16 @@ __device__ __forceinline__ void row_inverse_from(uint32_t (&v)[S::E], uint32_t* 
     }
 }
 
-// Dynamic shared memory of a row CTA: the row buffer and the buffer of operand a's transform
-// (4 bytes a residue each), then each row block's forward and inverse twiddles (8 bytes an entry,
-// N2 entries each).
-NC_HD constexpr size_t row_smem_bytes(int threads, int logE) { return size_t(threads) * (size_t(1) << logE) * 24; }
+// 512-thread row CTAs (two per SM) also prefetch operand b's residue block into shared memory;
+// 256-thread ones (four per SM) have no room left for it.
+NC_HD constexpr bool row_prefetch_b(int threads) { return threads == 512; }
+
+// Dynamic shared memory of a row CTA: the row buffer, the buffer of operand a's transform and,
+// with row_prefetch_b, b's residue block (4 bytes a residue each), then each row block's forward
+// and inverse twiddles (8 bytes an entry, N2 entries each).
+NC_HD constexpr size_t row_smem_bytes(int threads, int logE) {
+    return size_t(threads) * (size_t(1) << logE) * (row_prefetch_b(threads) ? 28 : 24);
+}
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
@@ -278,9 +284,12 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
     const uint32_t p = __ldg(&t.pc32[i].p), pinv = __ldg(&t.pc32[i].pinv);
     const int base = (1 << logN1) + u;
     const size_t off = size_t(i) * N + size_t(u) * S::N2;
+    constexpr bool PF_B = row_prefetch_b(THREADS);
+    constexpr int NBUF = PF_B ? 3 : 2;
     uint32_t* buf = reinterpret_cast<uint32_t*>(smem) + rr * S::N2;
     uint32_t* buf_a = reinterpret_cast<uint32_t*>(smem) + size_t(ROWS) * S::N2 + rr * S::N2;
-    uint2* s_twf = reinterpret_cast<uint2*>(smem + size_t(2) * ROWS * S::N2 * 4) + size_t(rr) * 2 * S::N2;
+    uint32_t* b_in = reinterpret_cast<uint32_t*>(smem) + size_t(2) * ROWS * S::N2 + rr * S::N2;  // with PF_B
+    uint2* s_twf = reinterpret_cast<uint2*>(smem + size_t(NBUF) * ROWS * S::N2 * 4) + size_t(rr) * 2 * S::N2;
     uint2* s_twi = s_twf + S::N2;
     const uint2* twf = t.fwd32 + size_t(i) * kMaxN;
     const uint2* twi = t.inv32 + size_t(i) * kMaxN;
@@ -291,7 +300,9 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
     uint32_t v[S::E];
 
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(ROWS) : "memory");
+        // one arrival per row for its twiddles and, for blocks of four or more, one for its residues
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(LOG_N2 >= 2 ? 2 * ROWS : ROWS)
+                     : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -318,20 +329,64 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
     };
 
     pdl_wait();  // the residues come from the stream's previous kernel
-    if (d.mode == kModeCachedA) {
-        const uint32_t* a_hat = reinterpret_cast<const uint32_t*>(d.a_hat);
+    // the residue blocks as bulk copies too (16-byte aligned for blocks of 4 and more): product
+    // and forward modes put a's block in buf_a and (with PF_B) b's in b_in; cached-a mode a_hat's
+    // block in buf and b's in buf_a. They are read in the first pass's layout, before any thread
+    // writes those buffers again.
+    constexpr bool BULK = LOG_N2 >= 2;
+    const uint32_t* a_src = d.mode == kModeCachedA ? reinterpret_cast<const uint32_t*>(d.a_hat) + off : ra + off;
+    uint32_t* a_dst = d.mode == kModeCachedA ? buf : buf_a;
+    uint32_t* b_dst = d.mode == kModeCachedA ? buf_a : b_in;
+    const bool b_bulk = d.mode == kModeCachedA || (PF_B && d.mode == kModeProduct);
+    if (BULK && lt == 0) {
+        asm volatile("fence.proxy.async.global;" ::: "memory");  // the previous kernel's writes -> bulk reads
+        const uint32_t bytes = (b_bulk ? 2u : 1u) * 4u * uint32_t(S::N2);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(a_dst)),
+                     "l"(a_src), "r"(4u * S::N2), "r"(bar)
+                     : "memory");
+        if (b_bulk)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             smem_addr(b_dst)),
+                         "l"(rb_res + off), "r"(4u * S::N2), "r"(bar)
+                         : "memory");
+    }
+    if (!BULK) {
+        // blocks of fewer than four residues: plain loads into the same places
 #pragma unroll
         for (int e = 0; e < S::E; ++e) {
             const int x = row_index<S, 0>(lt, e);
-            buf_a[swz(x)] = active ? __ldcg(a_hat + off + x) : 0u;
+            a_dst[x] = __ldcg(a_src + x);
+            if (b_bulk) b_dst[x] = __ldcg(rb_res + off + x);
         }
+    }
+    twiddles_ready();
+    if (BULK && !staged) {
+        // the bulk copies gave up: each row's threads load its blocks themselves
+        for (int x = lt; x < S::N2; x += S::T) {
+            a_dst[x] = __ldcg(a_src + x);
+            if (b_bulk) b_dst[x] = __ldcg(rb_res + off + x);
+        }
+        __syncthreads();
+    }
+    if (d.mode == kModeCachedA) {
+        // b's residues to registers, then a_hat from its raw block into buf_a in the last pass's
+        // swizzled layout (b's raw block, also in buf_a, is read first)
+        uint32_t av[S::E];
 #pragma unroll
-        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(rb_res + off + row_index<S, 0>(lt, e)) : 0u;
-        twiddles_ready();
+        for (int e = 0; e < S::E; ++e) {
+            const int x = row_index<S, 0>(lt, e);
+            v[e] = buf_a[x];
+            av[e] = buf[x];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) buf_a[swz(row_index<S, 0>(lt, e))] = av[e];
     } else {
 #pragma unroll
-        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(ra + off + row_index<S, 0>(lt, e)) : 0u;
-        twiddles_ready();
+        for (int e = 0; e < S::E; ++e) v[e] = buf_a[row_index<S, 0>(lt, e)];
+        if constexpr (S::NPASS == 1) __syncthreads();  // buf_a's raw block is read before it is rewritten
         row_forward_from<S, 0>(v, buf, s_twf, 1, lt, p);
         if (d.mode == kModeForward) {
             __syncthreads();
@@ -347,8 +402,13 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
             return;
         }
         row_store<S, LAST>(v, buf_a, lt);
+        if constexpr (PF_B) {
 #pragma unroll
-        for (int e = 0; e < S::E; ++e) v[e] = active ? __ldcg(rb_res + off + row_index<S, 0>(lt, e)) : 0u;
+            for (int e = 0; e < S::E; ++e) v[e] = b_in[row_index<S, 0>(lt, e)];
+        } else {
+#pragma unroll
+            for (int e = 0; e < S::E; ++e) v[e] = __ldcg(rb_res + off + row_index<S, 0>(lt, e));
+        }
     }
     row_forward_from<S, 0>(v, buf, s_twf, 1, lt, p);
     __syncthreads();
