@@ -679,14 +679,17 @@ def chained(dev, reps: int = 10) -> dict:
             ms_chain = _flushed_ms(run_chain, flush, reps)
             ms_pairs = _flushed_ms(run_pairs, flush, reps)
             exact = bool(torch.equal(c_chain, c_pair))
-            k_chain, k_pair = chain.k, pair.k
+            k_chain, k_pair, word_pair = chain.k, pair.plain_primes, pair.word_bits
         if not exact:
             raise RuntimeError(f"chained and pairwise products differ (m={m}, {bits}-bit q)")
         out[f"m{m}_q{bits}"] = {"chain_us": 1e3 * ms_chain, "pairwise_us": 1e3 * ms_pairs,
                                 "speedup": ms_pairs / ms_chain, "primes_chain": k_chain,
-                                "primes_pairwise": k_pair, "bit_exact_vs_pairwise": exact}
-    out["form"] = ("N=65536, device-resident; pairwise = m - 1 plain products, each output the next "
-                   "product's operand; L2 flushed before each timed run; median of 10")
+                                "primes_pairwise": k_pair, "pairwise_word_bits": word_pair,
+                                "bit_exact_vs_pairwise": exact}
+    out["form"] = ("N=65536, device-resident; pairwise = m - 1 plain products (the plan's engine: 30-bit "
+                   "where it runs), each output the next product's operand; the chain runs the 62-bit engine "
+                   "(its bound needs more than 64 primes below 2^30); L2 flushed before each timed run; "
+                   "median of 10")
     return out
 
 

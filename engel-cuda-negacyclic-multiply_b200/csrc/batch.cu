@@ -96,14 +96,11 @@ void Batch::finalize(cudaStream_t stream) {
     std::vector<uint64_t> shape;
     size_t scratch = 0;
     int kmax = 1, kmax_imad = 0, kmax_tc = 0;
-    // products that fill the GPU alone run the plain path's launches, on the plan's 30-bit engine
-    // where it runs (plain products whose residue scratch comes from the batch's arena)
-    auto direct_w32 = [](const Entry& e) {
-        return e.plan->logN >= kDirectLogN && e.mode == kModeProduct && !e.scratch && e.plan->use_w32();
-    };
+    // plain products whose residue scratch comes from the batch's arena run on the plan's 30-bit
+    // engine where it runs
+    auto on_w32 = [](const Entry& e) { return e.mode == kModeProduct && !e.scratch && e.plan->use_w32(); };
     auto residue_bytes = [&](const Entry& e) {
-        return round_up(direct_w32(e) ? e.plan->residue_bytes() : size_t(e.plan->k) * e.plan->N * sizeof(uint64_t),
-                        256);
+        return round_up(on_w32(e) ? e.plan->residue_bytes() : size_t(e.plan->k) * e.plan->N * sizeof(uint64_t), 256);
     };
     for (size_t p = 0; p < n; ++p) {
         const Plan* pl = entries_[p].plan;
@@ -120,6 +117,9 @@ void Batch::finalize(cudaStream_t stream) {
     }
     std::vector<uint2> dec, row, crt, crt_tc, dec_tc[kMaxLogN1 + 1];
     std::vector<uint2> row_by_size[kBatchRowLogMax + 1];
+    std::vector<uint2> crt_tc32, dec_tc32[kMaxLogN1 + 1], row32_by_size[kBatchRowLogMax + 1];
+    kmax32_ = 1;
+    lw_tc32_ = 2;
     direct_.clear();
     int lw_tc = 2;
     size_t off = 0;
@@ -145,7 +145,7 @@ void Batch::finalize(cudaStream_t stream) {
         }
         if (pl->logN >= kDirectLogN) {
             // fills the GPU alone: the plain path's launches with the plan's row configuration
-            const bool w32 = direct_w32(e);
+            const bool w32 = on_w32(e);
             const RowConfig& dc = w32 ? pl->cfg32 : pl->cfg;
             if (w32) {
                 ProductDesc dw = pl->desc_plain(e.a, e.b, e.c);
@@ -161,6 +161,29 @@ void Batch::finalize(cudaStream_t stream) {
             continue;
         }
         BatchProduct& bp = prods[p];
+        if (on_w32(e)) {
+            // the 30-bit engine: residue items on the tensor cores, row items by block size, CRT items
+            const Geometry g32 = geometry(pl->logN, pl->k32, cfg);
+            ProductDesc dw = pl->desc_plain(e.a, e.b, e.c);
+            dw.ra = d.ra;
+            dw.rb = d.rb;
+            dw.logN2 = uint32_t(cfg.logN2);
+            bp.d = dw;
+            bp.tiles = uint32_t(g32.tiles);
+            bp.first_operand = 0;
+            bp.tiles_tc = uint32_t(pl->N < kDecTcRows ? 1 : pl->N / kDecTcRows);
+            bp.n_dec = 0;
+            bp.n_row = uint32_t(g32.row_ctas);
+            const uint32_t pid = uint32_t(p);
+            for (uint32_t i = 0; i < 2 * bp.tiles_tc; ++i) dec_tc32[g32.logN1].push_back(make_uint2(pid, i));
+            for (uint32_t i = 0; i < bp.n_row; ++i) row32_by_size[cfg.logN2].push_back(make_uint2((kItemRow << 28) | pid, i));
+            for (uint32_t i = 0; i < uint32_t(g32.tiles); ++i) crt_tc32.push_back(make_uint2(pid, i));
+            kmax32_ = std::max(kmax32_, pl->k32);
+            lw_tc32_ = std::max(lw_tc32_, int(dw.LW));
+            shape.push_back((uint64_t(1) << 61) | (uint64_t(pl->logN) << 40) | (uint64_t(pl->k32) << 32) |
+                            (uint64_t(pl->L) << 8));
+            continue;
+        }
         bp.d = d;
         bp.tiles = uint32_t(g.tiles);
         bp.first_operand = e.mode == kModeCachedA ? 1u : 0u;
@@ -218,10 +241,29 @@ void Batch::finalize(cudaStream_t stream) {
         shape.push_back((uint64_t(l) << 32) | uint64_t(n_dec_tc_[l]));
     }
     shape.push_back(uint64_t(kmax_tc));
+    // the 30-bit products' items
+    row_groups32_.clear();
+    for (int l = kBatchRowLogMax; l >= 1; --l) {
+        if (row32_by_size[l].empty()) continue;
+        row_groups32_.push_back(RowGroup{l, int(items.size()), int(row32_by_size[l].size()), 0});
+        items.insert(items.end(), row32_by_size[l].begin(), row32_by_size[l].end());
+        shape.push_back((uint64_t(5) << 60) | (uint64_t(l) << 32) | uint64_t(row32_by_size[l].size()));
+    }
+    n_crt_tc32_ = int(crt_tc32.size());
+    crt32_first_ = int(items.size());
+    items.insert(items.end(), crt_tc32.begin(), crt_tc32.end());
+    dec32_first_ = int(items.size());
+    for (int l = 0; l <= kMaxLogN1; ++l) {
+        n_dec_tc32_[l] = int(dec_tc32[l].size());
+        items.insert(items.end(), dec_tc32[l].begin(), dec_tc32[l].end());
+        shape.push_back((uint64_t(6) << 60) | (uint64_t(l) << 32) | uint64_t(n_dec_tc32_[l]));
+    }
+    shape.push_back((uint64_t(7) << 60) | (uint64_t(kmax32_) << 32) | (uint64_t(lw_tc32_) << 16) |
+                    uint64_t(n_crt_tc32_));
 
     ensure(reinterpret_cast<char**>(&d_products_), &products_cap_, n * sizeof(BatchProduct), "batch products");
     ensure(&d_items_, &items_cap_, items.size(), "batch items");
-    ensure(&d_state_, &state_cap_, 2 * n + 5 + kBatchRowLogMax, "batch counters");
+    ensure(&d_state_, &state_cap_, 2 * n + 5 + 2 * kBatchRowLogMax, "batch counters");
     // Stream-ordered upload from pinned memory: the kernel on `stream` sees the tables only after
     // the copies (a synchronous copy from pageable memory may return before its DMA lands, and
     // nothing would order it before a launch on a non-blocking stream). The previous run has
@@ -262,6 +304,11 @@ void Batch::finalize(cudaStream_t stream) {
             g.ctas = std::max(1, std::min(per_sm * sms, g.count));
             ctas_ = std::max(ctas_, g.ctas);
         }
+    }
+    for (RowGroup& g : row_groups32_) {
+        check(persistent_rows32_occupancy(g.logN2, &per_sm), "occupancy");
+        g.ctas = std::max(1, std::min(per_sm * sms, g.count));
+        ctas_ = std::max(ctas_, g.ctas);
     }
     if (shape != shape_) {
         if (exec_) cudaGraphExecDestroy(exec_);
@@ -325,6 +372,29 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
         }
         if (e == cudaSuccess && n_crt_tc_ > 0) e = launch_batch_crt(tc, true, smem_crt_tc_, s);
         if (e == cudaSuccess && n_crt_ > 0) e = launch_batch_crt(im, false, smem_crt_, s);
+        // the 30-bit products: residue launches, persistent row launches, the CRT launch
+        int at32 = dec32_first_;
+        for (int l = 0; l <= kMaxLogN1 && e == cudaSuccess; ++l) {
+            if (n_dec_tc32_[l] == 0) continue;
+            BatchCrtArgs dt = tc;
+            dt.items = d_items_ + at32;
+            dt.n_items = n_dec_tc32_[l];
+            e = launch_batch_dec_tc32(dt, l, kmax32_, s);
+            at32 += n_dec_tc32_[l];
+        }
+        for (size_t g = 0; g < row_groups32_.size() && e == cudaSuccess; ++g) {
+            BatchArgs ga = args;
+            ga.items = d_items_ + row_groups32_[g].first;
+            ga.n_items = row_groups32_[g].count;
+            ga.head = d_state_ + 2 * n + 5 + kBatchRowLogMax + g;
+            e = launch_persistent_rows32(ga, row_groups32_[g].logN2, row_groups32_[g].ctas, s);
+        }
+        if (e == cudaSuccess && n_crt_tc32_ > 0) {
+            BatchCrtArgs ct = tc;
+            ct.items = d_items_ + crt32_first_;
+            ct.n_items = n_crt_tc32_;
+            e = launch_batch_crt_tc32(ct, lw_tc32_, s);
+        }
         if (!direct_.empty()) {
             // join the side stream back into s (also after a failed launch, so a capture ends whole)
             cudaError_t j = cudaEventRecord(join_, side_);
@@ -333,7 +403,7 @@ void Batch::run(cudaStream_t stream, bool use_graph) {
         }
         return e;
     };
-    const size_t state_bytes = (2 * n + 5 + kBatchRowLogMax) * sizeof(uint32_t);
+    const size_t state_bytes = (2 * n + 5 + 2 * kBatchRowLogMax) * sizeof(uint32_t);
     if (!use_graph) {
         check(cudaMemsetAsync(d_state_, 0, state_bytes, stream), "batch reset");
         check(enqueue(stream), "batch launch");

@@ -18,8 +18,11 @@ namespace nc {
 // row stage (and any residue items on the integer pipes), then one CRT launch per CRT engine in
 // use. Products of N >= 2^15 fill the GPU on their own: they run the plain path's launches with
 // their plan's row configuration, alternating between two streams so that one product's last
-// wave overlaps the next one's kernels. The counter reset and the launches are captured once into
-// a CUDA graph and replayed while the batch keeps the same shape.
+// wave overlaps the next one's kernels. Plain products (a, b -> c) of plans on the 30-bit word
+// engine run on it (residue scratch from the batch's arena): below 2^15 in their own residue,
+// persistent-row and CRT launches after the 62-bit ones, from 2^15 as the plain path's launches.
+// The counter reset and the launches are captured once into a CUDA graph and replayed while the
+// batch keeps the same shape.
 class Batch {
   public:
     explicit Batch(int device);
@@ -44,6 +47,8 @@ class Batch {
                 (n_crt_ > 0 ? 1 : 0);
         for (int c : n_dec_tc_) n += c > 0 ? 1 : 0;
         for (const Direct& x : direct_) n += x.d.mode == kModeForward ? 2 : 3;
+        n += int(row_groups32_.size()) + (n_crt_tc32_ > 0 ? 1 : 0);
+        for (int c : n_dec_tc32_) n += c > 0 ? 1 : 0;
         return n;
     }
     // After the last run has completed (its event): did a dependency wait give up?
@@ -101,6 +106,15 @@ class Batch {
     size_t smem_crt_tc_ = 0, smem_crt_ = 0;
     int n_dec_tc_[kMaxLogN1 + 1] = {};  // tensor-core residue items by log2 N1, after the CRT items
     size_t smem_dec_tc_ = 0;
+    // Products on the 30-bit engine (plain products of plans that use it, residue scratch from the
+    // batch's arena), after the items above in d_items_: their row items by row-block size (one
+    // persistent launch each; heads after the 62-bit groups'), their CRT items, their residue items
+    // by log2 N1.
+    std::vector<RowGroup> row_groups32_;
+    int n_crt_tc32_ = 0;
+    int n_dec_tc32_[kMaxLogN1 + 1] = {};
+    int crt32_first_ = 0, dec32_first_ = 0;  // positions in d_items_
+    int kmax32_ = 1, lw_tc32_ = 2;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
     cudaEvent_t done_ = nullptr;  // recorded after every run

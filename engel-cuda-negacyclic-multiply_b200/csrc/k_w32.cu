@@ -549,15 +549,136 @@ __global__ void __launch_bounds__(kThreads, 2) k_crt_tc32(ProductDesc d, Tables 
 template <int LOG_N2, int LOG_E, int THREADS>
 __global__ void __launch_bounds__(THREADS, (THREADS == 256 ? (LOG_E == 3 ? 4 : 3) : 2)) k_row32(ProductDesc d, Tables t) {
     extern __shared__ __align__(16) uint8_t smem[];
-    __shared__ uint64_t tw_bar;
+    __shared__ uint64_t bar;
     pdl_trigger();
-    w32::row_blocks<LOG_N2, LOG_E, THREADS>(d, t, int(blockIdx.x), smem, &tw_bar);
+    const uint32_t b = smem_u32(&bar);
+    w32::row_barrier_init<LOG_N2, LOG_E, THREADS>(b);
+    w32::row_blocks<LOG_N2, LOG_E, THREADS>(d, t, int(blockIdx.x), smem, b, 0, true);
 }
 
 #define NC_ROW32_VARIANTS(X)                                                                                   \
     X(1, 4, 256) X(2, 4, 256) X(3, 4, 256) X(4, 4, 256) X(5, 4, 256) X(6, 4, 256) X(7, 4, 256) X(8, 4, 256)  \
     X(9, 4, 256) X(10, 4, 256) X(11, 4, 256) X(12, 4, 256) X(6, 3, 256) X(7, 3, 256) X(8, 3, 256)           \
     X(9, 3, 256) X(10, 3, 256) X(11, 3, 256) X(12, 3, 512)
+
+// ------------------------------------------------------------------------------------------
+// batches (products of N < 2^15 on the 30-bit engine; batch.cu): the residue items of every such
+// product (one CTA per item), then one persistent row launch per row-block size, then the CRT
+// items. The launches of a batch run in stream order, so no item waits on another.
+
+// Residue items (x = product, y = operand * tiles_tc + tile), every product of the launch with
+// column length 2^LOG_N1.
+template <int LOG_N1>
+__global__ void __launch_bounds__(kThreads, 4) k_batch_dec_tc32(BatchCrtArgs a) {
+#if NC_HAS_TCGEN05
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t taddr_slot;
+    const uint2 w = __ldg(a.items + blockIdx.x);
+    const BatchProduct& bp = a.products[w.x];
+    const int tiles = int(bp.tiles_tc);
+    const int operand = int(bp.first_operand) + int(w.y) / tiles, tile = int(w.y) % tiles;
+    if (bp.d.logN >= 7)
+        dec_tc32_item<LOG_N1, (kDecTcRows >> LOG_N1)>(bp.d, a.tables, operand, tile, smem, bar, taddr_slot);
+    else
+        dec_tc32_item<LOG_N1, 0>(bp.d, a.tables, operand, tile, smem, bar, taddr_slot);
+#endif
+}
+
+// Row items (x = product, y = row-CTA index) with row blocks of 2^LOG_N2, radix 8, 256 threads:
+// persistent CTAs take items in queue order; each item's twiddles and residue blocks arrive on the
+// CTA's mbarrier, one phase per item. If a bulk wait gives up (the item then loads its data with
+// plain loads), the CTA's later items use plain loads too.
+template <int LOG_N2>
+__global__ void __launch_bounds__(kThreads, 4) k_persistent_rows32(BatchArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ int s_item;
+    __shared__ __align__(16) BatchProduct s_bp;
+    constexpr int kWords = int(sizeof(BatchProduct) / 4);
+    pdl_trigger();
+    const uint32_t b = smem_u32(&bar);
+    row_barrier_init<LOG_N2, kBatchRowLogE, kThreads>(b);
+    uint32_t parity = 0;
+    bool bulk = true;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = int(atomicAdd(a.head, 1u));
+        __syncthreads();
+        const int it = s_item;
+        if (it >= a.n_items) break;
+        const uint2 w = __ldg(a.items + it);
+        if (threadIdx.x < kWords)
+            reinterpret_cast<uint32_t*>(&s_bp)[threadIdx.x] =
+                __ldg(reinterpret_cast<const uint32_t*>(a.products + (w.x & 0x0fffffffu)) + threadIdx.x);
+        __syncthreads();
+        const bool ok = row_blocks<LOG_N2, kBatchRowLogE, kThreads>(s_bp.d, a.tables, int(w.y), smem, b, parity, bulk);
+        if (bulk) parity ^= 1u;
+        bulk = bulk && ok;  // the item's result stands either way; later items avoid the barrier
+        __syncthreads();  // s_item and s_bp are rewritten by the next round
+    }
+}
+
+// CRT items (x = product, y = 256-coefficient tile); products of at most 30 limbs (256 columns of
+// tensor memory per CTA).
+__global__ void __launch_bounds__(kThreads, 2) k_batch_crt_tc32(BatchCrtArgs a) {
+#if NC_HAS_TCGEN05
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t taddr_slot;
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(&taddr_slot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    pdl_trigger();  // only once the CTA holds its tensor memory
+    const uint32_t taddr = taddr_slot;
+    const uint2 w = __ldg(a.items + blockIdx.x);
+    const BatchProduct& bp = a.products[w.x];
+    switch (bp.d.LW) {
+#define NC_B_CRT_TC32(n)                                                        \
+    case n:                                                                     \
+        if constexpr (crt_tc_tmem_cols(n) == 256)                               \
+            crt32_coeffs_tc<n>(bp.d, a.tables, int(w.y), smem, taddr, &bar, 0); \
+        break;
+        NC_LW_CASES(NC_B_CRT_TC32)
+#undef NC_B_CRT_TC32
+        default: break;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(taddr) : "memory");
+#endif
+}
+
+void* batch_dec_tc32_kernel(int logN1) {
+    switch (logN1) {
+        case 0: return reinterpret_cast<void*>(&k_batch_dec_tc32<0>);
+        case 1: return reinterpret_cast<void*>(&k_batch_dec_tc32<1>);
+        case 2: return reinterpret_cast<void*>(&k_batch_dec_tc32<2>);
+        case 3: return reinterpret_cast<void*>(&k_batch_dec_tc32<3>);
+        case 4: return reinterpret_cast<void*>(&k_batch_dec_tc32<4>);
+        case 5: return reinterpret_cast<void*>(&k_batch_dec_tc32<5>);
+        default: return nullptr;
+    }
+}
+
+void* persistent_rows32_kernel(int logN2) {
+    switch (logN2) {
+#define NC_P_ROWS32(n) \
+    case n: return reinterpret_cast<void*>(&k_persistent_rows32<n>);
+        NC_P_ROWS32(1) NC_P_ROWS32(2) NC_P_ROWS32(3) NC_P_ROWS32(4) NC_P_ROWS32(5) NC_P_ROWS32(6)
+        NC_P_ROWS32(7) NC_P_ROWS32(8) NC_P_ROWS32(9) NC_P_ROWS32(10) NC_P_ROWS32(11)
+#undef NC_P_ROWS32
+        default: return nullptr;
+    }
+}
 
 void* dec_tc32_kernel(int logN1) {
     switch (logN1) {
@@ -621,7 +742,46 @@ cudaError_t prepare_w32() {
     for (int lw = 2; lw <= kMaxL && e == cudaSuccess; lw += 2)
         e = cudaFuncSetAttribute(w32::crt_tc32_kernel(lw), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(w32::crt_tc32_smem_bytes(lw)));
+    for (int l = 0; l <= kMaxLogN1 && e == cudaSuccess; ++l)
+        e = cudaFuncSetAttribute(w32::batch_dec_tc32_kernel(l), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(dec_tc32_smem_bytes(kMaxPrimes32)));
+    for (int n = 1; n <= kBatchRowLogMax && e == cudaSuccess; ++n)
+        e = cudaFuncSetAttribute(w32::persistent_rows32_kernel(n), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(w32::row_smem_bytes(kThreads, kBatchRowLogE)));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(w32::k_batch_crt_tc32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(w32::crt_tc32_smem_bytes(30)));
     return e;
+}
+
+cudaError_t launch_batch_dec_tc32(const BatchCrtArgs& args, int logN1, int kmax, cudaStream_t s) {
+    void* fn = w32::batch_dec_tc32_kernel(logN1);
+    if (!fn) return cudaErrorInvalidValue;
+    BatchCrtArgs a = args;
+    void* params[] = {&a};
+    return launch_pdl(fn, args.n_items, kThreads, dec_tc32_smem_bytes(kmax), s, params);
+}
+
+cudaError_t launch_persistent_rows32(const BatchArgs& args, int logN2, int ctas, cudaStream_t s) {
+    void* fn = w32::persistent_rows32_kernel(logN2);
+    if (!fn) return cudaErrorInvalidValue;
+    BatchArgs a = args;
+    void* params[] = {&a};
+    return launch_pdl(fn, ctas, kThreads, w32::row_smem_bytes(kThreads, kBatchRowLogE), s, params);
+}
+
+cudaError_t persistent_rows32_occupancy(int logN2, int* ctas_per_sm) {
+    void* fn = w32::persistent_rows32_kernel(logN2);
+    if (!fn) return cudaErrorInvalidValue;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, kThreads,
+                                                         w32::row_smem_bytes(kThreads, kBatchRowLogE));
+}
+
+cudaError_t launch_batch_crt_tc32(const BatchCrtArgs& args, int lw_max, cudaStream_t s) {
+    BatchCrtArgs a = args;
+    void* params[] = {&a};
+    return launch_pdl(reinterpret_cast<void*>(&w32::k_batch_crt_tc32), args.n_items, kThreads,
+                      w32::crt_tc32_smem_bytes(lw_max), s, params);
 }
 
 cudaError_t launch_residues32(const ProductDesc& d, const Tables& t, int logN1, cudaStream_t s, int first, int count,

@@ -66,5 +66,12 @@ cudaError_t launch_residues32(const ProductDesc& d, const Tables& t, int logN1, 
                               int tile0, int tiles);
 cudaError_t launch_row32(const ProductDesc& d, const Tables& t, const RowConfig& cfg, cudaStream_t s);
 cudaError_t launch_crt32(const ProductDesc& d, const Tables& t, int tiles, cudaStream_t s);
+// Batches on the 30-bit engine: residue items of products with column length 2^logN1 (kmax: the
+// most primes among them); row items of one row-block size on `ctas` persistent CTAs; CRT items
+// (lw_max: the widest LW among them, at most 30).
+cudaError_t launch_batch_dec_tc32(const BatchCrtArgs& args, int logN1, int kmax, cudaStream_t s);
+cudaError_t launch_persistent_rows32(const BatchArgs& args, int logN2, int ctas, cudaStream_t s);
+cudaError_t persistent_rows32_occupancy(int logN2, int* ctas_per_sm);
+cudaError_t launch_batch_crt_tc32(const BatchCrtArgs& args, int lw_max, cudaStream_t s);
 
 }  // namespace nc

@@ -263,13 +263,29 @@ __device__ __forceinline__ void copy_twiddles(const uint2* tw, int base, uint2* 
 // One CTA of THREADS threads handles THREADS / T row blocks, as row_blocks of stages.cuh: block
 // rb = item * ROWS + (tid / T) is prime rb >> logN1, row u = rb & (N1 - 1). Modes: product
 // (forward a and b, pointwise, inverse), cached-a (a's transform read from a_hat), forward (a's
-// transform written to hat_out). Residues are k x N u32. The twiddles of each row block are staged
-// in shared memory at the start (bulk copies on the CTA's mbarrier `tw_bar`, overlapping the
-// residue loads): the passes then wait on no global load but the residues. One launch per CTA
-// (the mbarrier's phase 0).
+// transform written to hat_out). Residues are k x N u32. The twiddles and the residue blocks of
+// each row block are staged in shared memory at the start by bulk copies that complete on the
+// CTA's mbarrier `bar` (row_barrier_init), phase `parity` (a persistent CTA's items alternate
+// phases): the passes then wait on no global load. use_bulk false (a persistent CTA after a bulk
+// wait gave up) loads them with plain loads instead. Returns false if this item's bulk wait gave
+// up (its data then came by plain loads, so the item's result stands).
 template <int LOG_N2, int LOG_E, int THREADS>
-__device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t, int item, uint8_t* smem,
-                                           uint64_t* tw_bar) {
+__device__ __forceinline__ void row_barrier_init(uint32_t bar) {
+    using S = RowShape<LOG_N2, LOG_E>;
+    constexpr int ROWS = THREADS / S::T;
+    if (threadIdx.x == 0) {
+        // per item: one arrival per row for its twiddles and, for blocks of four and more, one for
+        // its residue blocks
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(LOG_N2 >= 2 ? 2 * ROWS : ROWS)
+                     : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+template <int LOG_N2, int LOG_E, int THREADS>
+__device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t, int item, uint8_t* smem,
+                                           uint32_t bar, uint32_t parity, bool use_bulk) {
     using S = RowShape<LOG_N2, LOG_E>;
     static_assert(S::T <= THREADS, "row block needs more threads than the CTA has");
     constexpr int ROWS = THREADS / S::T;
@@ -295,18 +311,11 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
     const uint2* twi = t.inv32 + size_t(i) * kMaxN;
     const uint32_t* ra = reinterpret_cast<const uint32_t*>(d.ra);
     const uint32_t* rb_res = reinterpret_cast<const uint32_t*>(d.rb);
-    const uint32_t bar = smem_addr(tw_bar);
     const bool inverse = d.mode != kModeForward;
     uint32_t v[S::E];
 
-    if (threadIdx.x == 0) {
-        // one arrival per row for its twiddles and, for blocks of four or more, one for its residues
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(LOG_N2 >= 2 ? 2 * ROWS : ROWS)
-                     : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (lt == 0) {
+    __syncthreads();  // shared memory of a previous item is free
+    if (use_bulk && lt == 0) {
         // the twiddle tables do not depend on the previous kernel: their copies start before its end
         const uint32_t bytes = (inverse ? 2u : 1u) * 8u * ((1u << LOG_N2) - 2u);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -314,10 +323,10 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
         if (inverse) stage_twiddles<LOG_N2>(twi, base, s_twi, bar);
     }
     // every thread waits for the copies (bounded); if any gave up, each row's threads copy its
-    // twiddles themselves and, before the CTA exits, wait once more for the copies in flight
-    bool staged = true;
+    // twiddles themselves and, before the item ends, wait once more for the copies in flight
+    bool staged = use_bulk;
     auto twiddles_ready = [&] {
-        staged = __syncthreads_and(bar_wait(bar, 0) ? 1 : 0) != 0;
+        if (use_bulk) staged = __syncthreads_and(bar_wait(bar, parity) ? 1 : 0) != 0;
         if (!staged) {
             copy_twiddles<LOG_N2>(twf, base, s_twf, lt, S::T);
             if (inverse) copy_twiddles<LOG_N2>(twi, base, s_twi, lt, S::T);
@@ -325,7 +334,8 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
         }
     };
     auto finish = [&] {
-        if (!staged) bar_wait(bar, 0);
+        if (use_bulk && !staged) bar_wait(bar, parity);
+        return staged || !use_bulk;
     };
 
     pdl_wait();  // the residues come from the stream's previous kernel
@@ -338,7 +348,7 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
     uint32_t* a_dst = d.mode == kModeCachedA ? buf : buf_a;
     uint32_t* b_dst = d.mode == kModeCachedA ? buf_a : b_in;
     const bool b_bulk = d.mode == kModeCachedA || (PF_B && d.mode == kModeProduct);
-    if (BULK && lt == 0) {
+    if (BULK && use_bulk && lt == 0) {
         asm volatile("fence.proxy.async.global;" ::: "memory");  // the previous kernel's writes -> bulk reads
         const uint32_t bytes = (b_bulk ? 2u : 1u) * 4u * uint32_t(S::N2);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -363,7 +373,7 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
     }
     twiddles_ready();
     if (BULK && !staged) {
-        // the bulk copies gave up: each row's threads load its blocks themselves
+        // no bulk copies, or they gave up: each row's threads load its blocks themselves
         for (int x = lt; x < S::N2; x += S::T) {
             a_dst[x] = __ldcg(a_src + x);
             if (b_bulk) b_dst[x] = __ldcg(rb_res + off + x);
@@ -398,8 +408,7 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
 #pragma unroll
                 for (int e = 0; e < S::E; ++e) __stcg(out + off + row_index<S, 0>(lt, e), v[e]);
             }
-            finish();
-            return;
+            return finish();
         }
         row_store<S, LAST>(v, buf_a, lt);
         if constexpr (PF_B) {
@@ -423,7 +432,7 @@ __device__ __forceinline__ void row_blocks(const ProductDesc& d, const Tables& t
 #pragma unroll
         for (int e = 0; e < S::E; ++e) __stcg(out + off + row_index<S, 0>(lt, e), v[e]);
     }
-    finish();
+    return finish();
 }
 
 }  // namespace w32

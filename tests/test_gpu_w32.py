@@ -115,3 +115,44 @@ def test_w32_autotune_keeps_results_exact(gpu):
         assert plan.autotune(reps=2) > 0
         assert plan.row_config in nc.row_variants(16, word_bits=plan.word_bits)
         assert np.array_equal(plan.multiply(c.a, c.b), oracle.negacyclic(c.N, c.q_limbs, c.a, c.b))
+
+
+def test_w32_batches_mix_engines_and_modes(gpu):
+    """One batch holding plain products of 30-bit plans (their own residue, row and CRT launches),
+    the same products on 62-bit plans, a cached-a product of a 30-bit plan (62-bit NTT-domain
+    operand) and a product of N = 2^16 (plain launches), replayed from its graph twice."""
+    import torch
+
+    specs = [(1024, 868), (4096, 500), (16384, 868), (2048, 950), (65536, 868), (64, 300)]
+    with nc.Batch() as fwd, nc.Batch() as batch:
+        plans, checks = [], []
+        for j, (N, bits) in enumerate(specs):
+            c = cases.make_case(N, bits, seed=1300 + j, edge_frac=0.02)
+            want = oracle.negacyclic(N, c.q_limbs, c.a, c.b)
+            for bits_word in (32, 64):
+                p = nc.Plan(N, c.q_limbs, word_bits=bits_word)
+                plans.append(p)
+                da, db = _dev(c.a, gpu), _dev(c.b, gpu)
+                dc = da.new_zeros(da.shape)
+                batch.add(p, da.data_ptr(), db.data_ptr(), dc.data_ptr())
+                checks.append((dc, want, (N, bits, bits_word), (da, db)))
+            if N == 16384:
+                p = plans[-2]  # the 30-bit plan: its NTT-domain operands stay 62-bit (hat_words u64)
+                ahat = torch.empty(p.hat_words, dtype=torch.int64, device=gpu)
+                da_f = _dev(c.a, gpu)
+                fwd.add_forward(p, da_f.data_ptr(), ahat.data_ptr())
+                fwd.run(0, True)
+                fwd.synchronize()
+                db = _dev(c.b, gpu)
+                dc = db.new_zeros(db.shape)
+                batch.add_cached(p, ahat.data_ptr(), db.data_ptr(), dc.data_ptr())
+                checks.append((dc, want, (N, bits, "cached"), (ahat, db, da_f)))
+        for _ in range(2):
+            for dc, _, _, _ in checks:
+                dc.fill_(-1)
+            batch.run(0, True)
+            batch.synchronize()
+            for dc, want, what, _ in checks:
+                assert np.array_equal(_host(dc).reshape(want.shape), want), what
+        for p in plans:
+            p.close()
