@@ -755,10 +755,11 @@ def uneven_batch(dev, mix, args) -> dict:
     import cases
     import negacyclic as nc
 
-    plans, bufs = [], []
+    plans, bufs, engines = [], [], []
     for i, (N, bits, q) in enumerate(mix):
         L = (bits + 31) // 32
         p = nc.Plan(N, cases.limbs_of(q, L))
+        engines.append((p.plain_primes, p.word_bits))
         x = torch.from_numpy(cases.coeffs(q, N, L, 11000 + i).view(np.int32)).to(dev)
         y = torch.from_numpy(cases.coeffs(q, N, L, 12000 + i).view(np.int32)).to(dev)
         plans.append(p)
@@ -783,10 +784,8 @@ def uneven_batch(dev, mix, args) -> dict:
     if not exact:
         raise RuntimeError("uneven batch differs from plain products")
     total_imad = 0.0
-    for N, bits, _ in mix:
-        L = (bits + 31) // 32
-        k = 29 if bits > 600 else 15
-        total_imad += sum(stage_work(k, N, L))
+    for (N, bits, _), (k, word) in zip(mix, engines):
+        total_imad += sum(stage_work(k, N, (bits + 31) // 32, None, word))
     return {"products": len(mix), "mix": "N log-uniform 2^10..2^16, q 434- or 868-bit (seeded per product)",
             "batched": {"value": len(mix) / (ms_batch * 1e-3), "unit": "products/s", "ms_per_launch": ms_batch,
                         "ctas": info["ctas"], "imad_alg_rate_gops": total_imad / (ms_batch * 1e-3) / 1e9},

@@ -77,6 +77,12 @@ int nc_self_check(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q) {
         if (!host.empty()) throw nc::Error(nc::kESelfCheck, "init self-check: " + host);
         const std::string qerr = nc::check_qconst(c);
         if (!qerr.empty()) throw nc::Error(nc::kESelfCheck, "init self-check of the plan's constants: " + qerr);
+        // the 30-bit engine's constants, where its 64 primes cover the bound
+        nc::QConst32 c32{};
+        if (nc::build_qconst32(q, int(L), logN, &c32).empty()) {
+            const std::string e32 = nc::check_qconst32(c32);
+            if (!e32.empty()) throw nc::Error(nc::kESelfCheck, "init self-check of the plan's 30-bit constants: " + e32);
+        }
     });
 }
 
@@ -219,6 +225,14 @@ int nc_primes(uint64_t* out, int count) {
         if (!out || count < 0 || count > nc::kMaxPrimes) throw nc::Error(nc::kEInval, "count must be 0..48");
         const auto& ps = nc::prime_set();
         for (int i = 0; i < count; ++i) out[i] = ps[i].p;
+    });
+}
+
+int nc_primes32(uint32_t* out, int count) {
+    return guarded([&] {
+        if (!out || count < 0 || count > nc::kMaxPrimes32) throw nc::Error(nc::kEInval, "count must be 0..64");
+        const auto& ps = nc::prime_set32();
+        for (int i = 0; i < count; ++i) out[i] = ps[size_t(i)].p;
     });
 }
 

@@ -49,6 +49,7 @@ C_SYMBOLS = [
     ("nc_plan_stage_ms", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float)]),
     ("nc_imad_peak", ctypes.c_int, [ctypes.POINTER(ctypes.c_double)]),
     ("nc_primes", ctypes.c_int, [_u64p, ctypes.c_int]),
+    ("nc_primes32", ctypes.c_int, [_u32p, ctypes.c_int]),
     ("nc_residues", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
     ("nc_residues_status", ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     ("nc_plan_set_residue_engine", ctypes.c_int, [_vp, ctypes.c_int]),
@@ -132,6 +133,13 @@ def imad_peak() -> float:
 def primes(count: int = 48) -> list[int]:
     out = (ctypes.c_uint64 * count)()
     _check(load().nc_primes(out, count))
+    return list(out)
+
+
+def primes32(count: int = 64) -> list[int]:
+    """The 30-bit word engine's primes (below 2^30, 1 mod 2^17, descending)."""
+    out = (ctypes.c_uint32 * count)()
+    _check(load().nc_primes32(out, count))
     return list(out)
 
 

@@ -51,7 +51,8 @@ int nc_plan_create(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, nc_pla
    the host arithmetic, the prime set and a sample of every prime's tables (once per process), then
    the plan's CRT constants: y_i (M/p_i) N = 1 mod p_i from an independent product of the other
    primes, (M/p_i mod q) p_i + ((-M) mod q) = 0 mod q for every i, the Barrett constant's defining
-   inequality, and the Shoup companions. They hold for every valid q. Returns NC_OK, NC_EINVAL for
+   inequality, and the Shoup companions; the same for the 30-bit word engine's constants where its
+   primes cover the bound (y_i (M/p_i) N = 2^32 mod p_i). They hold for every valid q. Returns NC_OK, NC_EINVAL for
    an invalid point, or NC_ESELFCHECK. nc_plan_create runs the same checks and, once per device,
    an N = 8 known-answer product on the device. Mirrors the self-checks of the reference's
    fherma_init (solve.cu:1151-1165, 1285-1314, 1370-1415), without its L = 28 Barrett check,
@@ -116,7 +117,8 @@ int nc_plan_get_crt_engine(const nc_plan* plan);
 /* Waits for the plan's own stream (the one nc_multiply uses). */
 int nc_plan_synchronize(nc_plan* plan);
 
-/* N, L, number of residue primes k, and bit length of q. Any pointer may be NULL. */
+/* N, L, number of residue primes k of the 62-bit engine (nc_plan_word_bits gives the engine in
+   use and its count), and bit length of q. Any pointer may be NULL. */
 int nc_plan_query(const nc_plan* plan, uint32_t* N, uint32_t* L, uint32_t* k, uint32_t* qbits);
 
 /* Device milliseconds from the first kernel of the last nc_multiply to its last (CUDA events).
@@ -137,6 +139,8 @@ int nc_imad_peak(double* ops_per_second);
 
 /* Residue primes of the fixed set (p = 2^62 - m, p = 1 mod 2^17), first `count` of 48. */
 int nc_primes(uint64_t* out, int count);
+/* The 30-bit word engine's primes (p < 2^30, p = 1 mod 2^17, descending), first `count` of 64. */
+int nc_primes32(uint32_t* out, int count);
 
 /* ------------------------------------------------------------------ residue-stage ablation
  *

@@ -38,3 +38,26 @@ def test_self_check_rejects_invalid_points(N, limbs, W, msg):
     with pytest.raises(nc.NegacyclicError, match=msg) as ei:
         nc.self_check(N, np.array(limbs, dtype=np.uint32), W=W)
     assert ei.value.code == nc.NC_EINVAL
+
+
+def test_thirty_bit_prime_set():
+    """The 30-bit engine's primes: 64 distinct primes below 2^30 (above 2^29), 1 mod 2^17, descending;
+    the reference's bound picks 59 of them for an 868-bit q at N = 2^16 and all 64 reach 948 bits."""
+    ps = nc.primes32(64)
+    assert len(ps) == 64 and ps == sorted(ps, reverse=True) and len(set(ps)) == 64
+    for p in ps:
+        assert (1 << 29) < p < (1 << 30) and (p - 1) % (1 << 17) == 0
+        assert all(pow(a, p - 1, p) == 1 for a in (2, 3, 5, 7, 11, 13))
+
+    def needed(log_n, bits):
+        prod, k = 1, 0
+        while prod.bit_length() < log_n + 2 * bits + 4:
+            prod *= ps[k]
+            k += 1
+        return k
+
+    assert needed(16, 868) == 59
+    prod = 1
+    for p in ps:
+        prod *= p
+    assert (prod.bit_length() - 16 - 4) // 2 == 948
