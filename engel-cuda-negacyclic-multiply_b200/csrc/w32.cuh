@@ -44,6 +44,15 @@ __device__ __forceinline__ void gs_bfly(uint32_t& x, uint32_t& y, uint32_t w, ui
     y = shoup(d, w, wq, p);
 }
 
+// The inverse butterfly with twiddle -w: (x, y) -> (x + y, (y - x) w). The row stage's inverse
+// twiddles are negated forward ones (below), so it takes the forward pair unchanged.
+__device__ __forceinline__ void gs_bfly_neg(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p, uint32_t p2) {
+    const uint32_t s = csub(x + y, p2);
+    const uint32_t d = y - x + p2;
+    x = s;
+    y = shoup(d, w, wq, p);
+}
+
 // a b 2^-32 mod p in [0, 2p) for a < p, b < 4p (Montgomery; pinv = -p^-1 mod 2^32): the sum
 // a b + m p stays below 2^63 and its high word below p (4 p^2 / 2^32) + p.
 __device__ __forceinline__ uint32_t mont(uint32_t a, uint32_t b, uint32_t p, uint32_t pinv) {
@@ -103,8 +112,15 @@ __device__ __forceinline__ void column_inverse_root(const uint2* tw, int root, u
 // ------------------------------------------------------------------------------------------
 // row blocks: the register passes of stages.cuh over u32 residues
 
+// One pass of R stages over the thread's groups. tw is a row block's staged twiddles (local
+// stage l at tw[(1 << l) + t], stage_twiddles). Forward passes take entry t of the row block's
+// forward table; inverse passes take the staged forward twiddles of the mirrored row block in
+// reverse order: the inverse twiddle of node 2^s + j of the merged tree, psi^-bitrev(2^s + j),
+// equals -psi^bitrev(2^s + (2^s - 1 - j)) (psi^N = -1), and for a row block u of N1 at local
+// stage l, j = u 2^l + t mirrors to (N1 - 1 - u) 2^l + (2^l - 1 - t). The 2^j twiddles of a
+// stage are adjacent, so pairs of them load as one 16-byte access.
 template <class S, int PASS, bool FWD>
-__device__ __forceinline__ void row_pass(uint32_t (&v)[S::E], const uint2* tw, int base, int lt, uint32_t p) {
+__device__ __forceinline__ void row_pass(uint32_t (&v)[S::E], const uint2* tw, int lt, uint32_t p) {
     constexpr int R = S::r(PASS), LL = S::lolog(PASS), L0 = S::l0(PASS);
     const uint32_t p2 = 2 * p;
 #pragma unroll
@@ -115,17 +131,43 @@ __device__ __forceinline__ void row_pass(uint32_t (&v)[S::E], const uint2* tw, i
         for (int jj = 0; jj < R; ++jj) {
             const int j = FWD ? jj : R - 1 - jj;
             const int half = 1 << (R - 1 - j);
-            const int twbase = (base << (L0 + j)) + (hi << j);
+            uint2 w[1 << (R - 1)];
+            if (FWD) {
+                // entries (1 << l) + hi 2^j + blk
+                const int first = (1 << (L0 + j)) + (hi << j);
+                if (j == 0) {
+                    w[0] = tw[first];
+                } else {
+#pragma unroll
+                    for (int b2 = 0; b2 < (1 << j); b2 += 2) {
+                        const uint4 pr = reinterpret_cast<const uint4*>(tw)[(first + b2) >> 1];
+                        w[b2] = make_uint2(pr.x, pr.y);
+                        w[b2 + 1] = make_uint2(pr.z, pr.w);
+                    }
+                }
+            } else {
+                // entries (2 << l) - 1 - hi 2^j - blk (descending in blk)
+                const int last = (2 << (L0 + j)) - 1 - (hi << j);
+                if (j == 0) {
+                    w[0] = tw[last];
+                } else {
+#pragma unroll
+                    for (int b2 = 0; b2 < (1 << j); b2 += 2) {
+                        const uint4 pr = reinterpret_cast<const uint4*>(tw)[(last - b2 - 1) >> 1];
+                        w[b2] = make_uint2(pr.z, pr.w);
+                        w[b2 + 1] = make_uint2(pr.x, pr.y);
+                    }
+                }
+            }
 #pragma unroll
             for (int blk = 0; blk < (1 << j); ++blk) {
-                const uint2 w = tw[twbase + blk];  // shared memory (stage_twiddles)
 #pragma unroll
                 for (int s0 = 0; s0 < half; ++s0) {
                     const int e = q * (1 << R) + blk * 2 * half + s0;
                     if (FWD)
-                        ct_bfly(v[e], v[e + half], w.x, w.y, p, p2);
+                        ct_bfly(v[e], v[e + half], w[blk].x, w[blk].y, p, p2);
                     else
-                        gs_bfly(v[e], v[e + half], w.x, w.y, p, p2);
+                        gs_bfly_neg(v[e], v[e + half], w[blk].x, w[blk].y, p, p2);
                 }
             }
         }
@@ -179,28 +221,26 @@ __device__ __forceinline__ void row_load(uint32_t (&v)[S::E], const uint32_t* bu
 }
 
 template <class S, int PASS>
-__device__ __forceinline__ void row_forward_from(uint32_t (&v)[S::E], uint32_t* buf, const uint2* tw, int base, int lt,
-                                                 uint32_t p) {
-    row_pass<S, PASS, true>(v, tw, base, lt, p);
+__device__ __forceinline__ void row_forward_from(uint32_t (&v)[S::E], uint32_t* buf, const uint2* tw, int lt, uint32_t p) {
+    row_pass<S, PASS, true>(v, tw, lt, p);
     if constexpr (PASS + 1 < S::NPASS) {
         __syncthreads();
         row_store<S, PASS>(v, buf, lt);
         __syncthreads();
         row_load<S, PASS + 1>(v, buf, lt);
-        row_forward_from<S, PASS + 1>(v, buf, tw, base, lt, p);
+        row_forward_from<S, PASS + 1>(v, buf, tw, lt, p);
     }
 }
 
 template <class S, int PASS>
-__device__ __forceinline__ void row_inverse_from(uint32_t (&v)[S::E], uint32_t* buf, const uint2* tw, int base, int lt,
-                                                 uint32_t p) {
-    row_pass<S, PASS, false>(v, tw, base, lt, p);
+__device__ __forceinline__ void row_inverse_from(uint32_t (&v)[S::E], uint32_t* buf, const uint2* tw, int lt, uint32_t p) {
+    row_pass<S, PASS, false>(v, tw, lt, p);
     if constexpr (PASS > 0) {
         __syncthreads();
         row_store<S, PASS>(v, buf, lt);
         __syncthreads();
         row_load<S, PASS - 1>(v, buf, lt);
-        row_inverse_from<S, PASS - 1>(v, buf, tw, base, lt, p);
+        row_inverse_from<S, PASS - 1>(v, buf, tw, lt, p);
     }
 }
 
@@ -298,7 +338,10 @@ __device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t
     const int i = active ? rb >> logN1 : 0;
     const int u = rb & ((1 << logN1) - 1);
     const uint32_t p = __ldg(&t.pc32[i].p), pinv = __ldg(&t.pc32[i].pinv);
+    // node of the row block in the merged tree, and of its mirror (N1 - 1 - u), whose forward
+    // twiddles serve as the inverse ones (row_pass)
     const int base = (1 << logN1) + u;
+    const int base_mirror = (2 << logN1) - 1 - u;
     const size_t off = size_t(i) * N + size_t(u) * S::N2;
     constexpr bool PF_B = row_prefetch_b(THREADS);
     constexpr int NBUF = PF_B ? 3 : 2;
@@ -308,7 +351,6 @@ __device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t
     uint2* s_twf = reinterpret_cast<uint2*>(smem + size_t(NBUF) * ROWS * S::N2 * 4) + size_t(rr) * 2 * S::N2;
     uint2* s_twi = s_twf + S::N2;
     const uint2* twf = t.fwd32 + size_t(i) * kMaxN;
-    const uint2* twi = t.inv32 + size_t(i) * kMaxN;
     const uint32_t* ra = reinterpret_cast<const uint32_t*>(d.ra);
     const uint32_t* rb_res = reinterpret_cast<const uint32_t*>(d.rb);
     const bool inverse = d.mode != kModeForward;
@@ -320,7 +362,7 @@ __device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t
         const uint32_t bytes = (inverse ? 2u : 1u) * 8u * ((1u << LOG_N2) - 2u);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
         stage_twiddles<LOG_N2>(twf, base, s_twf, bar);
-        if (inverse) stage_twiddles<LOG_N2>(twi, base, s_twi, bar);
+        if (inverse) stage_twiddles<LOG_N2>(twf, base_mirror, s_twi, bar);
     }
     // every thread waits for the copies (bounded); if any gave up, each row's threads copy its
     // twiddles themselves and, before the item ends, wait once more for the copies in flight
@@ -329,7 +371,7 @@ __device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t
         if (use_bulk) staged = __syncthreads_and(bar_wait(bar, parity) ? 1 : 0) != 0;
         if (!staged) {
             copy_twiddles<LOG_N2>(twf, base, s_twf, lt, S::T);
-            if (inverse) copy_twiddles<LOG_N2>(twi, base, s_twi, lt, S::T);
+            if (inverse) copy_twiddles<LOG_N2>(twf, base_mirror, s_twi, lt, S::T);
             __syncthreads();
         }
     };
@@ -397,7 +439,7 @@ __device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t
 #pragma unroll
         for (int e = 0; e < S::E; ++e) v[e] = buf_a[row_index<S, 0>(lt, e)];
         if constexpr (S::NPASS == 1) __syncthreads();  // buf_a's raw block is read before it is rewritten
-        row_forward_from<S, 0>(v, buf, s_twf, 1, lt, p);
+        row_forward_from<S, 0>(v, buf, s_twf, lt, p);
         if (d.mode == kModeForward) {
             __syncthreads();
             row_store<S, LAST>(v, buf, lt);
@@ -419,14 +461,14 @@ __device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t
             for (int e = 0; e < S::E; ++e) v[e] = __ldcg(rb_res + off + row_index<S, 0>(lt, e));
         }
     }
-    row_forward_from<S, 0>(v, buf, s_twf, 1, lt, p);
+    row_forward_from<S, 0>(v, buf, s_twf, lt, p);
     __syncthreads();
     const uint32_t p2 = 2 * p;
     uint32_t av[S::E];
     row_load<S, LAST>(av, buf_a, lt);
 #pragma unroll
     for (int e = 0; e < S::E; ++e) v[e] = mont(csub(csub(av[e], p2), p), v[e], p, pinv);
-    row_inverse_from<S, LAST>(v, buf, s_twi, 1, lt, p);
+    row_inverse_from<S, LAST>(v, buf, s_twi, lt, p);
     if (active) {
         uint32_t* out = reinterpret_cast<uint32_t*>(d.ra);
 #pragma unroll
