@@ -117,7 +117,8 @@ void Batch::finalize(cudaStream_t stream) {
     }
     std::vector<uint2> dec, row, crt, crt_tc, dec_tc[kMaxLogN1 + 1];
     std::vector<uint2> row_by_size[kBatchRowLogMax + 1];
-    std::vector<uint2> crt_tc32, dec_tc32[kMaxLogN1 + 1], row32_by_size[kBatchRowLogMax + 1];
+    std::vector<uint2> crt_tc32, dec_tc32[kMaxLogN1 + 1], row32_by_size[kBatchRowLogMax + 1],
+        row32_tail[kBatchRowLogMax + 1];
     kmax32_ = 1;
     lw_tc32_ = 2;
     direct_.clear();
@@ -176,7 +177,20 @@ void Batch::finalize(cudaStream_t stream) {
             bp.n_row = uint32_t(g32.row_ctas);
             const uint32_t pid = uint32_t(p);
             for (uint32_t i = 0; i < 2 * bp.tiles_tc; ++i) dec_tc32[g32.logN1].push_back(make_uint2(pid, i));
-            for (uint32_t i = 0; i < bp.n_row; ++i) row32_by_size[cfg.logN2].push_back(make_uint2((kItemRow << 28) | pid, i));
+            const int logN1_32 = pl->logN - cfg.logN2;
+            if (cfg.logN2 == kBatchRowLogMax && logN1_32 >= 1) {
+                // row pairs (k_persistent_rows32 takes two adjacent items): row blocks u and
+                // N1 - 1 - u of each prime next to each other, an even count per product
+                const uint32_t n1 = 1u << logN1_32;
+                for (uint32_t i = 0; i < uint32_t(pl->k32); ++i)
+                    for (uint32_t u = 0; u < n1 / 2; ++u) {
+                        row32_by_size[cfg.logN2].push_back(make_uint2((kItemRow << 28) | pid, i * n1 + u));
+                        row32_by_size[cfg.logN2].push_back(make_uint2((kItemRow << 28) | pid, i * n1 + n1 - 1 - u));
+                    }
+            } else {
+                // after every product's pairs, so that the pairs stay aligned to even positions
+                for (uint32_t i = 0; i < bp.n_row; ++i) row32_tail[cfg.logN2].push_back(make_uint2((kItemRow << 28) | pid, i));
+            }
             for (uint32_t i = 0; i < uint32_t(g32.tiles); ++i) crt_tc32.push_back(make_uint2(pid, i));
             kmax32_ = std::max(kmax32_, pl->k32);
             lw_tc32_ = std::max(lw_tc32_, int(dw.LW));
@@ -244,6 +258,7 @@ void Batch::finalize(cudaStream_t stream) {
     // the 30-bit products' items
     row_groups32_.clear();
     for (int l = kBatchRowLogMax; l >= 1; --l) {
+        row32_by_size[l].insert(row32_by_size[l].end(), row32_tail[l].begin(), row32_tail[l].end());
         if (row32_by_size[l].empty()) continue;
         row_groups32_.push_back(RowGroup{l, int(items.size()), int(row32_by_size[l].size()), 0});
         items.insert(items.end(), row32_by_size[l].begin(), row32_by_size[l].end());

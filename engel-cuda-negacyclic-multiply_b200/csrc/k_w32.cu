@@ -596,24 +596,53 @@ __global__ void __launch_bounds__(kThreads, 4) k_persistent_rows32(BatchArgs a) 
     __shared__ int s_item;
     __shared__ __align__(16) BatchProduct s_bp;
     constexpr int kWords = int(sizeof(BatchProduct) / 4);
+    // with one row block a CTA, items come two at a time: a mirror pair (adjacent in the queue,
+    // batch.cu) runs as row_pair, anything else as two row_blocks
+    constexpr bool kPairs = RowShape<LOG_N2, kBatchRowLogE>::T == kThreads;
     pdl_trigger();
     const uint32_t b = smem_u32(&bar);
     row_barrier_init<LOG_N2, kBatchRowLogE, kThreads>(b);
     uint32_t parity = 0;
     bool bulk = true;
+    auto load_product = [&](uint32_t x) {
+        if (threadIdx.x < kWords)
+            reinterpret_cast<uint32_t*>(&s_bp)[threadIdx.x] =
+                __ldg(reinterpret_cast<const uint32_t*>(a.products + (x & 0x0fffffffu)) + threadIdx.x);
+        __syncthreads();
+    };
+    auto single = [&](int y) {
+        const bool ok = row_blocks<LOG_N2, kBatchRowLogE, kThreads>(s_bp.d, a.tables, y, smem, b, parity, bulk);
+        if (bulk) parity ^= 1u;
+        bulk = bulk && ok;  // the item's result stands either way; later items avoid the barrier
+    };
     for (;;) {
-        if (threadIdx.x == 0) s_item = int(atomicAdd(a.head, 1u));
+        if (threadIdx.x == 0) s_item = int(atomicAdd(a.head, kPairs ? 2u : 1u));
         __syncthreads();
         const int it = s_item;
         if (it >= a.n_items) break;
         const uint2 w = __ldg(a.items + it);
-        if (threadIdx.x < kWords)
-            reinterpret_cast<uint32_t*>(&s_bp)[threadIdx.x] =
-                __ldg(reinterpret_cast<const uint32_t*>(a.products + (w.x & 0x0fffffffu)) + threadIdx.x);
-        __syncthreads();
-        const bool ok = row_blocks<LOG_N2, kBatchRowLogE, kThreads>(s_bp.d, a.tables, int(w.y), smem, b, parity, bulk);
-        if (bulk) parity ^= 1u;
-        bulk = bulk && ok;  // the item's result stands either way; later items avoid the barrier
+        load_product(w.x);
+        if constexpr (kPairs) {
+            const bool has2 = it + 1 < a.n_items;
+            const uint2 w2 = has2 ? __ldg(a.items + it + 1) : make_uint2(0u, 0u);
+            const int logN1 = int(s_bp.d.logN) - LOG_N2;
+            const int mask = (1 << logN1) - 1;
+            const int mirror = (int(w.y) & ~mask) | (mask - (int(w.y) & mask));
+            if (has2 && w2.x == w.x && logN1 >= 1 && int(w2.y) == mirror) {
+                // two phases when the copies ran, so the parity is unchanged
+                bulk = row_pair<LOG_N2, kBatchRowLogE, kThreads>(s_bp.d, a.tables, int(w.y), int(w2.y), smem, b, parity,
+                                                                 bulk, a.error, w.x);
+            } else {
+                single(int(w.y));
+                if (has2) {
+                    __syncthreads();  // s_bp is rewritten
+                    load_product(w2.x);
+                    single(int(w2.y));
+                }
+            }
+        } else {
+            single(int(w.y));
+        }
         __syncthreads();  // s_item and s_bp are rewritten by the next round
     }
 }

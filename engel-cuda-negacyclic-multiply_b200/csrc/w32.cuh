@@ -477,6 +477,145 @@ __device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t
     return finish();
 }
 
+// Row pairs of a batch's persistent row launch (plain products, one row block a row of the CTA):
+// row block u of a prime and its mirror u' = N1 - 1 - u in turn. The forward twiddles of u' read
+// in reverse are the inverse twiddles of u and the other way round (row_pass), so the pair's
+// twiddles are staged once, and u''s residue block of a arrives by a bulk copy issued once u's
+// pointwise product has read buf_a, while u's inverse runs: one staging wait for two blocks.
+// Mbarrier phases (two arrivals each, row_barrier_init): `parity` for the twiddles and u's block
+// of a, parity ^ 1 for the block of a of u'; b's blocks come by plain loads in the forward pass,
+// as in row_blocks without row_prefetch_b (with it, by bulk copies with a's). rb0 and rb1 are the
+// two row blocks (prime * N1 + u). Returns false if a bulk wait gave up (the blocks then came by
+// plain loads and the results stand); the caller then stops using the barrier. With use_bulk
+// false every block comes by plain loads. If the first member's copies have not landed after two
+// bounded waits, its buffers cannot safely take the second member's blocks: error[0] is set
+// (error[1] = what), which the host reports as a failed batch.
+template <int LOG_N2, int LOG_E, int THREADS>
+__device__ __forceinline__ bool row_pair(const ProductDesc& d, const Tables& t, int rb0, int rb1, uint8_t* smem,
+                                         uint32_t bar, uint32_t parity, bool use_bulk, uint32_t* error, uint32_t what) {
+    using S = RowShape<LOG_N2, LOG_E>;
+    static_assert(S::T == THREADS && LOG_N2 >= 2, "row pairs take one row block a CTA, staged by bulk copies");
+    constexpr int LAST = S::NPASS - 1;
+    constexpr bool PF_B = row_prefetch_b(THREADS);
+    constexpr int NBUF = PF_B ? 3 : 2;
+    const int logN1 = int(d.logN) - LOG_N2;
+    const int N = 1 << d.logN;
+    const int lt = int(threadIdx.x);
+    const int i = rb0 >> logN1;
+    const int u0 = rb0 & ((1 << logN1) - 1), u1 = rb1 & ((1 << logN1) - 1);
+    const uint32_t p = __ldg(&t.pc32[i].p), pinv = __ldg(&t.pc32[i].pinv);
+    uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* buf_a = buf + S::N2;
+    uint32_t* b_in = buf + 2 * S::N2;  // with PF_B
+    uint2* const s_tw0 = reinterpret_cast<uint2*>(smem + size_t(NBUF) * S::N2 * 4);
+    uint2* const s_tw1 = s_tw0 + S::N2;
+    const uint2* twf = t.fwd32 + size_t(i) * kMaxN;
+    const uint32_t* ra = reinterpret_cast<const uint32_t*>(d.ra);
+    const uint32_t* rbr = reinterpret_cast<const uint32_t*>(d.rb);
+    uint32_t* out = reinterpret_cast<uint32_t*>(d.ra);
+    const size_t off0 = size_t(i) * N + size_t(u0) * S::N2, off1 = size_t(i) * N + size_t(u1) * S::N2;
+    constexpr uint32_t kBlockBytes = (PF_B ? 8u : 4u) * S::N2;
+    // lt 0: one arrival expecting the blocks of a (and b) of the member at `off`, and their copies
+    auto copy_blocks = [&](size_t off) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kBlockBytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(buf_a)),
+                     "l"(ra + off), "r"(4u * S::N2), "r"(bar)
+                     : "memory");
+        if constexpr (PF_B)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             smem_addr(b_in)),
+                         "l"(rbr + off), "r"(4u * S::N2), "r"(bar)
+                         : "memory");
+    };
+    // the same blocks by plain loads, every thread
+    auto load_blocks = [&](size_t off) {
+        for (int x = lt; x < S::N2; x += S::T) {
+            buf_a[x] = __ldcg(ra + off + x);
+            if constexpr (PF_B) b_in[x] = __ldcg(rbr + off + x);
+        }
+    };
+
+    __syncthreads();  // shared memory of a previous item is free
+    if (use_bulk && lt == 0) {
+        // the twiddles do not depend on the previous kernel: their copies start before its end
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(16u * ((1u << LOG_N2) - 2u))
+                     : "memory");
+        stage_twiddles<LOG_N2>(twf, (1 << logN1) + u0, s_tw0, bar);
+        stage_twiddles<LOG_N2>(twf, (1 << logN1) + u1, s_tw1, bar);
+    }
+    pdl_wait();  // the residues come from the stream's previous kernel
+    if (use_bulk && lt == 0) {
+        asm volatile("fence.proxy.async.global;" ::: "memory");  // the previous kernel's writes -> bulk reads
+        copy_blocks(off0);
+    }
+    // phase whose copies may still be in flight (-1: none) once a wait gave up
+    int pending = -1;
+    bool staged = use_bulk && __syncthreads_and(bar_wait(bar, parity) ? 1 : 0) != 0;
+    if (!staged) {
+        if (use_bulk) pending = 0;
+        copy_twiddles<LOG_N2>(twf, (1 << logN1) + u0, s_tw0, lt, S::T);
+        copy_twiddles<LOG_N2>(twf, (1 << logN1) + u1, s_tw1, lt, S::T);
+        load_blocks(off0);
+        __syncthreads();
+    }
+    const uint32_t p2 = 2 * p;
+#pragma unroll 1
+    for (int j = 0; j < 2; ++j) {
+        const size_t off = j ? off1 : off0;
+        if (j == 1) {
+            if (staged) {
+                staged = __syncthreads_and(bar_wait(bar, parity ^ 1u) ? 1 : 0) != 0;
+                if (!staged) pending = 1;
+            } else if (pending == 0) {
+                // once the late copies of the first member are done, its buffers are free
+                if (__syncthreads_and(bar_wait(bar, parity) ? 1 : 0) != 0)
+                    pending = -1;
+                else if (error && lt == 0 && atomicCAS(error, 0u, 1u) == 0u)
+                    error[1] = what;
+            }
+            if (!staged) {
+                load_blocks(off1);
+                __syncthreads();
+            }
+        }
+        uint32_t v[S::E];
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) v[e] = buf_a[row_index<S, 0>(lt, e)];
+        if constexpr (S::NPASS == 1) __syncthreads();  // buf_a's raw block is read before it is rewritten
+        row_forward_from<S, 0>(v, buf, j ? s_tw1 : s_tw0, lt, p);
+        row_store<S, LAST>(v, buf_a, lt);
+        if constexpr (PF_B) {
+#pragma unroll
+            for (int e = 0; e < S::E; ++e) v[e] = b_in[row_index<S, 0>(lt, e)];
+        } else {
+#pragma unroll
+            for (int e = 0; e < S::E; ++e) v[e] = __ldcg(rbr + off + row_index<S, 0>(lt, e));
+        }
+        row_forward_from<S, 0>(v, buf, j ? s_tw1 : s_tw0, lt, p);
+        __syncthreads();
+        {
+            uint32_t av[S::E];
+            row_load<S, LAST>(av, buf_a, lt);
+#pragma unroll
+            for (int e = 0; e < S::E; ++e) v[e] = mont(csub(csub(av[e], p2), p), v[e], p, pinv);
+        }
+        if (j == 0) {
+            __syncthreads();  // every thread has read buf_a (and b_in)
+            if (staged && lt == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // those reads -> the bulk writes
+                copy_blocks(off1);
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+            }
+        }
+        row_inverse_from<S, LAST>(v, buf, j ? s_tw0 : s_tw1, lt, p);
+#pragma unroll
+        for (int e = 0; e < S::E; ++e) __stcg(out + off + row_index<S, 0>(lt, e), v[e]);
+    }
+    if (pending >= 0) bar_wait(bar, pending ? parity ^ 1u : parity);  // copies in flight end before the smem is reused
+    return use_bulk && pending < 0;
+}
+
 }  // namespace w32
 
 }  // namespace nc
