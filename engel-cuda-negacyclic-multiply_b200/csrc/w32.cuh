@@ -484,8 +484,8 @@ __device__ __forceinline__ bool row_blocks(const ProductDesc& d, const Tables& t
 // pointwise product has read buf_a, while u's inverse runs: one staging wait for two blocks.
 // Mbarrier phases (two arrivals each, row_barrier_init): `parity` for the twiddles and u's block
 // of a, parity ^ 1 for the block of a of u'; b's blocks come by plain loads in the forward pass,
-// as in row_blocks without row_prefetch_b (with it, by bulk copies with a's). rb0 and rb1 are the
-// two row blocks (prime * N1 + u). Returns false if a bulk wait gave up (the blocks then came by
+// as in row_blocks without row_prefetch_b (256-thread CTAs). rb0 and rb1 are the two row blocks
+// (prime * N1 + u). Returns false if a bulk wait gave up (the blocks then came by
 // plain loads and the results stand); the caller then stops using the barrier. With use_bulk
 // false every block comes by plain loads. If the first member's copies have not landed after two
 // bounded waits, its buffers cannot safely take the second member's blocks: error[0] is set
@@ -495,9 +495,8 @@ __device__ __forceinline__ bool row_pair(const ProductDesc& d, const Tables& t, 
                                          uint32_t bar, uint32_t parity, bool use_bulk, uint32_t* error, uint32_t what) {
     using S = RowShape<LOG_N2, LOG_E>;
     static_assert(S::T == THREADS && LOG_N2 >= 2, "row pairs take one row block a CTA, staged by bulk copies");
+    static_assert(!row_prefetch_b(THREADS), "row pairs load b's blocks in the forward pass");
     constexpr int LAST = S::NPASS - 1;
-    constexpr bool PF_B = row_prefetch_b(THREADS);
-    constexpr int NBUF = PF_B ? 3 : 2;
     const int logN1 = int(d.logN) - LOG_N2;
     const int N = 1 << d.logN;
     const int lt = int(threadIdx.x);
@@ -506,34 +505,24 @@ __device__ __forceinline__ bool row_pair(const ProductDesc& d, const Tables& t, 
     const uint32_t p = __ldg(&t.pc32[i].p), pinv = __ldg(&t.pc32[i].pinv);
     uint32_t* buf = reinterpret_cast<uint32_t*>(smem);
     uint32_t* buf_a = buf + S::N2;
-    uint32_t* b_in = buf + 2 * S::N2;  // with PF_B
-    uint2* const s_tw0 = reinterpret_cast<uint2*>(smem + size_t(NBUF) * S::N2 * 4);
+    uint2* const s_tw0 = reinterpret_cast<uint2*>(smem + size_t(2) * S::N2 * 4);
     uint2* const s_tw1 = s_tw0 + S::N2;
     const uint2* twf = t.fwd32 + size_t(i) * kMaxN;
     const uint32_t* ra = reinterpret_cast<const uint32_t*>(d.ra);
     const uint32_t* rbr = reinterpret_cast<const uint32_t*>(d.rb);
     uint32_t* out = reinterpret_cast<uint32_t*>(d.ra);
     const size_t off0 = size_t(i) * N + size_t(u0) * S::N2, off1 = size_t(i) * N + size_t(u1) * S::N2;
-    constexpr uint32_t kBlockBytes = (PF_B ? 8u : 4u) * S::N2;
-    // lt 0: one arrival expecting the blocks of a (and b) of the member at `off`, and their copies
+    // lt 0: one arrival expecting the block of a of the member at `off`, and its copy
     auto copy_blocks = [&](size_t off) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kBlockBytes) : "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(4u * S::N2) : "memory");
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                          smem_addr(buf_a)),
                      "l"(ra + off), "r"(4u * S::N2), "r"(bar)
                      : "memory");
-        if constexpr (PF_B)
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                             smem_addr(b_in)),
-                         "l"(rbr + off), "r"(4u * S::N2), "r"(bar)
-                         : "memory");
     };
-    // the same blocks by plain loads, every thread
+    // the same block by plain loads, every thread
     auto load_blocks = [&](size_t off) {
-        for (int x = lt; x < S::N2; x += S::T) {
-            buf_a[x] = __ldcg(ra + off + x);
-            if constexpr (PF_B) b_in[x] = __ldcg(rbr + off + x);
-        }
+        for (int x = lt; x < S::N2; x += S::T) buf_a[x] = __ldcg(ra + off + x);
     };
 
     __syncthreads();  // shared memory of a previous item is free
@@ -585,13 +574,8 @@ __device__ __forceinline__ bool row_pair(const ProductDesc& d, const Tables& t, 
         if constexpr (S::NPASS == 1) __syncthreads();  // buf_a's raw block is read before it is rewritten
         row_forward_from<S, 0>(v, buf, j ? s_tw1 : s_tw0, lt, p);
         row_store<S, LAST>(v, buf_a, lt);
-        if constexpr (PF_B) {
 #pragma unroll
-            for (int e = 0; e < S::E; ++e) v[e] = b_in[row_index<S, 0>(lt, e)];
-        } else {
-#pragma unroll
-            for (int e = 0; e < S::E; ++e) v[e] = __ldcg(rbr + off + row_index<S, 0>(lt, e));
-        }
+        for (int e = 0; e < S::E; ++e) v[e] = __ldcg(rbr + off + row_index<S, 0>(lt, e));
         row_forward_from<S, 0>(v, buf, j ? s_tw1 : s_tw0, lt, p);
         __syncthreads();
         {
@@ -601,7 +585,7 @@ __device__ __forceinline__ bool row_pair(const ProductDesc& d, const Tables& t, 
             for (int e = 0; e < S::E; ++e) v[e] = mont(csub(csub(av[e], p2), p), v[e], p, pinv);
         }
         if (j == 0) {
-            __syncthreads();  // every thread has read buf_a (and b_in)
+            __syncthreads();  // every thread has read buf_a
             if (staged && lt == 0) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // those reads -> the bulk writes
                 copy_blocks(off1);
