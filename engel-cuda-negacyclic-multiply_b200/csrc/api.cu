@@ -418,7 +418,8 @@ int nc_plan_autotune(nc_plan* plan, int reps, float* best_ms) {
 }
 
 uint64_t nc_plan_hat_words(const nc_plan* plan) {
-    return plan ? uint64_t(plan->p->k) * uint64_t(plan->p->N) : 0;
+    // k N u64 words on the 62-bit engine; k32 N u32 values on the 30-bit one (the larger of the two)
+    return plan ? uint64_t((plan->p->residue_bytes() + 7) / 8) : 0;
 }
 
 int nc_batch_create(nc_batch** out) {

@@ -96,9 +96,9 @@ void Batch::finalize(cudaStream_t stream) {
     std::vector<uint64_t> shape;
     size_t scratch = 0;
     int kmax = 1, kmax_imad = 0, kmax_tc = 0;
-    // plain products whose residue scratch comes from the batch's arena run on the plan's 30-bit
-    // engine where it runs
-    auto on_w32 = [](const Entry& e) { return e.mode == kModeProduct && !e.scratch && e.plan->use_w32(); };
+    // every entry of a plan that runs the 30-bit engine runs it here too (its NTT-domain operands
+    // are 30-bit residues, and caller scratch holds Plan::residue_bytes, enough for either engine)
+    auto on_w32 = [](const Entry& e) { return e.plan->use_w32(); };
     auto residue_bytes = [&](const Entry& e) {
         return round_up(on_w32(e) ? e.plan->residue_bytes() : size_t(e.plan->k) * e.plan->N * sizeof(uint64_t), 256);
     };
@@ -152,6 +152,9 @@ void Batch::finalize(cudaStream_t stream) {
                 ProductDesc dw = pl->desc_plain(e.a, e.b, e.c);
                 dw.ra = d.ra;
                 dw.rb = d.rb;
+                dw.mode = e.mode;
+                dw.a_hat = e.a_hat;
+                dw.hat_out = e.hat_out;
                 d = dw;
             }
             d.logN2 = uint32_t(dc.logN2);
@@ -169,16 +172,21 @@ void Batch::finalize(cudaStream_t stream) {
             dw.ra = d.ra;
             dw.rb = d.rb;
             dw.logN2 = uint32_t(cfg.logN2);
+            dw.mode = e.mode;
+            dw.a_hat = e.a_hat;
+            dw.hat_out = e.hat_out;
             bp.d = dw;
             bp.tiles = uint32_t(g32.tiles);
-            bp.first_operand = 0;
+            // operands with a residue stage: both (product), a (forward) or b (cached a)
+            bp.first_operand = e.mode == kModeCachedA ? 1u : 0u;
+            const uint32_t operands = e.mode == kModeProduct ? 2u : 1u;
             bp.tiles_tc = uint32_t(pl->N < kDecTcRows ? 1 : pl->N / kDecTcRows);
             bp.n_dec = 0;
             bp.n_row = uint32_t(g32.row_ctas);
             const uint32_t pid = uint32_t(p);
-            for (uint32_t i = 0; i < 2 * bp.tiles_tc; ++i) dec_tc32[g32.logN1].push_back(make_uint2(pid, i));
+            for (uint32_t i = 0; i < operands * bp.tiles_tc; ++i) dec_tc32[g32.logN1].push_back(make_uint2(pid, i));
             const int logN1_32 = pl->logN - cfg.logN2;
-            if (cfg.logN2 == kBatchRowLogMax && logN1_32 >= 1) {
+            if (e.mode == kModeProduct && cfg.logN2 == kBatchRowLogMax && logN1_32 >= 1) {
                 // row pairs (k_persistent_rows32 takes two adjacent items): row blocks u and
                 // N1 - 1 - u of each prime next to each other, an even count per product
                 const uint32_t n1 = 1u << logN1_32;
@@ -191,11 +199,12 @@ void Batch::finalize(cudaStream_t stream) {
                 // after every product's pairs, so that the pairs stay aligned to even positions
                 for (uint32_t i = 0; i < bp.n_row; ++i) row32_tail[cfg.logN2].push_back(make_uint2((kItemRow << 28) | pid, i));
             }
-            for (uint32_t i = 0; i < uint32_t(g32.tiles); ++i) crt_tc32.push_back(make_uint2(pid, i));
+            if (e.mode != kModeForward)
+                for (uint32_t i = 0; i < uint32_t(g32.tiles); ++i) crt_tc32.push_back(make_uint2(pid, i));
             kmax32_ = std::max(kmax32_, pl->k32);
             lw_tc32_ = std::max(lw_tc32_, int(dw.LW));
             shape.push_back((uint64_t(1) << 61) | (uint64_t(pl->logN) << 40) | (uint64_t(pl->k32) << 32) |
-                            (uint64_t(pl->L) << 8));
+                            (uint64_t(pl->L) << 8) | e.mode);
             continue;
         }
         bp.d = d;

@@ -628,7 +628,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_persistent_rows32(BatchArgs a) 
             const int logN1 = int(s_bp.d.logN) - LOG_N2;
             const int mask = (1 << logN1) - 1;
             const int mirror = (int(w.y) & ~mask) | (mask - (int(w.y) & mask));
-            if (has2 && w2.x == w.x && logN1 >= 1 && int(w2.y) == mirror) {
+            if (has2 && w2.x == w.x && s_bp.d.mode == kModeProduct && logN1 >= 1 && int(w2.y) == mirror) {
                 // two phases when the copies ran, so the parity is unchanged
                 bulk = row_pair<LOG_N2, kBatchRowLogE, kThreads>(s_bp.d, a.tables, int(w.y), int(w2.y), smem, b, parity,
                                                                  bulk, a.error, w.x);

@@ -128,7 +128,7 @@ int Server::register_operand(Plan* plan, const uint32_t* a) {
     if (plan->device != device_ || current_device() != device_)
         throw Error(kEInval, "the plan and the calling thread must be on the server's device");
     const size_t limb = granules(plan->limbs() * 4);
-    const size_t hat = granules(size_t(plan->k) * plan->N * 8);
+    const size_t hat = granules(plan->residue_bytes());  // either engine's NTT-domain form
     const size_t scratch = 2 * hat;
     char *dev_hat, *tmp;
     {
@@ -189,11 +189,12 @@ uint64_t Server::submit(Plan* plan, const uint32_t* a, int operand, const uint32
     r->plan = plan;
     r->operand = operand;
     r->limb_bytes = granules(plan->limbs() * 4);
-    r->dev_bytes = 3 * r->limb_bytes + 2 * granules(size_t(plan->k) * plan->N * 8);
+    r->dev_bytes = 3 * r->limb_bytes + 2 * granules(plan->residue_bytes());
     auto check_operand = [&]() -> std::map<int, Operand>::iterator {
         auto it = operands_.find(operand);
         if (it == operands_.end()) throw Error(kEInval, "unknown operand");
         if (it->second.plan->N != plan->N || it->second.plan->k != plan->k ||
+            it->second.plan->use_w32() != plan->use_w32() ||
             std::memcmp(it->second.plan->hq.q, plan->hq.q, sizeof(plan->hq.q)) != 0)
             throw Error(kEInval, "the operand was registered for another N or q");
         return it;

@@ -311,7 +311,8 @@ class Plan:
 
     @property
     def hat_words(self) -> int:
-        """u64 words of one operand's NTT-domain form (k * N)."""
+        """u64 words that hold one operand's NTT-domain form on either engine (k * N u64 on the
+        62-bit one, k32 * N u32 on the 30-bit one)."""
         return int(load().nc_plan_hat_words(self._h))
 
     def close(self) -> None:

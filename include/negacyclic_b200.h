@@ -233,7 +233,9 @@ int nc_batch_run(nc_batch* batch, void* stream, int use_graph);
 int nc_batch_synchronize(nc_batch* batch);
 /* Products, persistent CTAs of the last run, bytes of residue scratch held. Pointers may be NULL. */
 int nc_batch_query(const nc_batch* batch, uint32_t* products, uint32_t* ctas, uint64_t* scratch_bytes);
-/* u64 words of the NTT-domain form of one operand of this plan (k * N). */
+/* u64 words that hold the NTT-domain form of one operand of this plan on either engine: k * N u64
+   on the 62-bit engine, k32 * N u32 on the 30-bit one (the plan's engine decides which a batch's
+   forward and cached-a products use). */
 uint64_t nc_plan_hat_words(const nc_plan* plan);
 
 /* ------------------------------------------------------------------ serving

@@ -119,8 +119,9 @@ def test_w32_autotune_keeps_results_exact(gpu):
 
 def test_w32_batches_mix_engines_and_modes(gpu):
     """One batch holding plain products of 30-bit plans (their own residue, row and CRT launches),
-    the same products on 62-bit plans, a cached-a product of a 30-bit plan (62-bit NTT-domain
-    operand) and a product of N = 2^16 (plain launches), replayed from its graph twice."""
+    the same products on 62-bit plans, a cached-a product of a 30-bit plan (its NTT-domain operand
+    in 30-bit residues, from a forward batch) and a product of N = 2^16 (plain launches), replayed
+    from its graph twice."""
     import torch
 
     specs = [(1024, 868), (4096, 500), (16384, 868), (2048, 950), (65536, 868), (64, 300)]
@@ -137,7 +138,7 @@ def test_w32_batches_mix_engines_and_modes(gpu):
                 batch.add(p, da.data_ptr(), db.data_ptr(), dc.data_ptr())
                 checks.append((dc, want, (N, bits, bits_word), (da, db)))
             if N == 16384:
-                p = plans[-2]  # the 30-bit plan: its NTT-domain operands stay 62-bit (hat_words u64)
+                p = plans[-2]  # the 30-bit plan: hat_words covers its 30-bit NTT-domain form
                 ahat = torch.empty(p.hat_words, dtype=torch.int64, device=gpu)
                 da_f = _dev(c.a, gpu)
                 fwd.add_forward(p, da_f.data_ptr(), ahat.data_ptr())
